@@ -1,0 +1,411 @@
+#!/usr/bin/env python
+"""Benchmark of the split-operator Gross-Pitaevskii step on B200.
+
+Workload (the configuration the headline metric is quoted on): a 2D real-time
+rotating condensate, 1024^2 grid on [-16,16)^2, hbar = m = 1, wx = wy = 1,
+g = 500, rotation Omega = 0.7 as the gauge A = Omega(-y, x) applied by
+per-axis 1D FFT passes, dt = 5e-5.  The initial state is a seeded synthetic
+stand-in for "the FP64 ground state with a smoothed random phase": an FP64
+imaginary-time relaxation of the same Hamiltonian on the GPU (done before
+timing) times exp(i theta), theta = 2 pi U(0,1) smoothed by a Gaussian of width
+0.5 (seed 2).
+
+One bench step = 2 split-operator time steps (one full cycle of GPUE's
+alternating x/y gauge order), run by the fused complex64 form through the C
+ABI.  L2 (126 MB) is flushed by a 256 MiB write before every timed step;
+each step is timed with CUDA events on the library's stream.  The same
+protocol times the plain FP64 form for the fused-FP32 vs plain-FP64 ratio.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+--impl reference times GPUE's path on the host CPU: the reference has no CPU
+implementation, so this arm runs the FP64 CPU restatement of it (oracle/,
+OpenMP over all host threads) on the same workload.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("grid-point-steps/s fused-FP32 vs plain-FP64 (same B200, ΔE/E≤1e-6); "
+          "p99 lat")
+UNIT = "grid-point-steps/s"
+WORK = dict(dim=2, n=1024, box=16.0, wx=1.0, wy=1.0, g=500.0, omega=0.7, gauge=True,
+            dt=5e-5, gdt=1e-4, total_steps=20000)
+WORKLOAD_NAME = ("2D real-time rotating condensate 1024^2 on [-16,16)^2, g=500, Omega=0.7 "
+                 "gauge, dt=5e-5")
+STEPS_PER_BENCH_STEP = 2
+FLUSH_BYTES = 256 << 20
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="skip the steady-state and e2e legs")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------- inputs -------
+
+def phase_field(n, box, seed=2):
+    import numpy as np
+    dx = box / (n >> 1)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    theta = 2 * np.pi * rng.random((n, n))
+    k = 2 * np.pi * np.fft.fftfreq(n, d=dx)
+    k2 = k[:, None] ** 2 + k[None, :] ** 2
+    return np.real(np.fft.ifft2(np.fft.fft2(theta) * np.exp(-0.5 * k2 * 0.25)))
+
+
+def initial_state(G, device):
+    """FP64 imaginary-time relaxation (GPU) times a smoothed random phase."""
+    import numpy as np
+    n, box = WORK["n"], WORK["box"]
+    dx = box / (n >> 1)
+    x = -box + dx * np.arange(n)
+    r2 = x[None, :] ** 2 + x[:, None] ** 2
+    psi = np.exp(-r2 / 8.0).astype(np.complex128)
+    p = G.make_params(2, n, box, g=WORK["g"], omega=WORK["omega"], gauge=True, gdt=2e-3,
+                      dt=WORK["dt"], precision=G.PREC_FP64, device=device)
+    with G.Solver(p) as s:
+        s.set_wfc(psi)
+        s.evolve(5000, 0)
+        gs = s.get_wfc()
+    return np.ascontiguousarray(gs * np.exp(1j * phase_field(n, box)))
+
+
+def work_params(G, precision, device):
+    return G.make_params(2, WORK["n"], WORK["box"], wx=WORK["wx"], wy=WORK["wy"],
+                         g=WORK["g"], omega=WORK["omega"], gauge=True, gdt=WORK["gdt"],
+                         dt=WORK["dt"], precision=precision, device=device)
+
+
+# ------------------------------------------------------------ clocks ------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [t.strip() for t in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------- GPU timing -------
+
+def timed_steps(G, torch, s, steps, warmup, dev, flush, barrier, sampler=None):
+    """Per bench step: flush L2, then 2 time steps between CUDA events."""
+    stream = torch.cuda.ExternalStream(s.stream(), device=dev)
+    launches = 0
+    off = 0
+    for _ in range(warmup):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        s.evolve(STEPS_PER_BENCH_STEP, 1, no_sync=True, step_offset=off)
+        off += STEPS_PER_BENCH_STEP
+    torch.cuda.synchronize(dev)
+    barrier()
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    if sampler:
+        sampler.start()
+    for k in range(steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k & 7))
+            ev[k][0].record(stream)
+        r = s.evolve(STEPS_PER_BENCH_STEP, 1, no_sync=True, step_offset=off)
+        launches += r["kernel_launches"]
+        off += STEPS_PER_BENCH_STEP
+        with torch.cuda.stream(stream):
+            ev[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    clocks = sampler.stop() if sampler else None
+    barrier()
+    torch.cuda.synchronize(dev)
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    return ms, launches, clocks
+
+
+def steady_state(G, s, nsteps):
+    """One gpue_evolve call of nsteps (graph-replayed, no flushes)."""
+    r = s.evolve(nsteps, 1)
+    return r["device_ms"], r["kernel_launches"]
+
+
+def e2e_leg(G, torch, psi0, dev, calls=10, steps_per_call=100):
+    """Through the C ABI with pinned host buffers: upload psi (complex128),
+    evolve one printSteps-sized segment, download psi and the energy."""
+    import numpy as np
+    n = WORK["n"]
+    pin_in = torch.empty((n, n), dtype=torch.complex128, pin_memory=True)
+    pin_out = torch.empty((n, n), dtype=torch.complex128, pin_memory=True)
+    hin = pin_in.numpy()
+    hin[...] = psi0
+    hout = pin_out.numpy()
+    import ctypes as C
+    with G.Solver(work_params(G, G.PREC_FP32, dev)) as s:
+        stream = torch.cuda.ExternalStream(s.stream(), device=dev)
+        L = G.lib()
+        # warm the graphs once
+        L.gpue_set_wfc(s._h, C.c_void_p(hin.ctypes.data), G.MEM_HOST, G.C128)
+        s.evolve(steps_per_call, 1)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+        energies = []
+        off = 0
+        for _ in range(calls):
+            assert L.gpue_set_wfc(s._h, C.c_void_p(hin.ctypes.data), G.MEM_HOST, G.C128) == 0
+            s.evolve(steps_per_call, 1, no_sync=True, step_offset=off)
+            off += steps_per_call
+            assert L.gpue_get_wfc(s._h, C.c_void_p(hout.ctypes.data), G.MEM_HOST, G.C128) == 0
+            energies.append(s.energy())
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1)
+    pts = n * n
+    return {"value": pts * steps_per_call * calls / (ms * 1e-3), "unit": UNIT,
+            "h2d_bytes_per_step": pts * 16, "d2h_bytes_per_step": pts * 16 + 8,
+            "step": "one gpue_evolve() call of %d time steps (GPUE's default printSteps) "
+                    "with psi uploaded from pinned host memory before it and psi plus the "
+                    "energy read back after it" % steps_per_call,
+            "calls": calls, "ms": ms}
+
+
+def accuracy_leg(G, psi0, dev, nsteps=2000):
+    """Energy drift of the fused FP32 form against the plain FP64 form over
+    nsteps real-time steps from the same state (the FP64 form is pinned to
+    GPUE's own build by the parity tests)."""
+    out = {}
+    for name, prec in (("fp64", G.PREC_FP64), ("fp32", G.PREC_FP32)):
+        with G.Solver(work_params(G, prec, dev)) as s:
+            s.set_wfc(psi0)
+            s.evolve(nsteps, 1)
+            out[name] = s.energy()
+    return {"steps": nsteps, "E_fp64": out["fp64"], "E_fp32": out["fp32"],
+            "dE_rel": abs(out["fp32"] - out["fp64"]) / abs(out["fp64"])}
+
+
+# ------------------------------------------------------------- CPU --------
+
+def cpu_oracle_rate(psi0, budget_s=12.0, threads=0):
+    """FP64 CPU restatement (oracle) on the same workload, bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    n = WORK["n"]
+    P = oracle.Problem(2, n, WORK["box"], g=WORK["g"], omega=WORK["omega"], gauge=True,
+                       dt=WORK["dt"], gdt=WORK["gdt"], threads=threads)
+    t = time.time()
+    P.evolve(psi0, 2, 1)
+    per = (time.time() - t) / 2
+    steps = max(2, min(2000, int(budget_s / max(per, 1e-6))))
+    steps += steps % 2
+    t = time.time()
+    P.evolve(psi0, steps, 1)
+    dt = time.time() - t
+    cores = threads or os.cpu_count()
+    return {"value": n * n * steps / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "%d real-time steps of the 1024^2 rotating case (FP64, OpenMP over "
+                      "lines, %d threads)" % (steps, cores), "seconds": dt}
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    n = WORK["n"]
+    dx = WORK["box"] / (n >> 1)
+    x = -WORK["box"] + dx * np.arange(n)
+    psi0 = (np.exp(-(x[None, :] ** 2 + x[:, None] ** 2) / 8.0) *
+            np.exp(1j * phase_field(n, WORK["box"]))).astype(np.complex128)
+    psi0 /= np.sqrt(np.sum(abs(psi0) ** 2) * dx * dx)
+    import oracle
+    P = oracle.Problem(2, n, WORK["box"], g=WORK["g"], omega=WORK["omega"], gauge=True,
+                       dt=WORK["dt"], gdt=WORK["gdt"])
+    budget = 150.0
+    psi = psi0
+    for _ in range(min(args.warmup, 2)):
+        psi, _, _ = P.evolve(psi, STEPS_PER_BENCH_STEP, 1)
+    t0 = time.time()
+    done = 0
+    while done < args.steps and time.time() - t0 < budget:
+        psi, _, _ = P.evolve(psi, STEPS_PER_BENCH_STEP, 1)
+        done += 1
+    secs = time.time() - t0
+    val = n * n * STEPS_PER_BENCH_STEP * done / secs
+    cores = os.cpu_count()
+    line = {"metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": done, "warmup": args.warmup, "ms_per_step": 1e3 * secs / max(done, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": WORKLOAD_NAME, "grid": n, "step": "2 time steps",
+                       "steps_requested": args.steps, "budget_s": budget},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": "%d bench steps (%d time steps) of the same workload "
+                                       "on the FP64 CPU restatement, OpenMP over %d threads"
+                                       % (done, done * STEPS_PER_BENCH_STEP, cores)},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------- main -------
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+    import torch
+    import gpue_b200 as G
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dev = local
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", dev))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    psi0 = initial_state(G, dev)
+    pts = WORK["n"] ** 2
+    res = {}
+    for name, prec in (("fp64", G.PREC_FP64), ("fp32", G.PREC_FP32)):
+        with G.Solver(work_params(G, prec, dev)) as s:
+            s.set_wfc(psi0)
+            sampler = ClockSampler(dev) if name == "fp32" else None
+            ms, launches, clocks = timed_steps(G, torch, s, args.steps, args.warmup, dev, flush,
+                                               barrier, sampler)
+            steady = None
+            if not args.quick:
+                sms, sl = steady_state(G, s, WORK["total_steps"])
+                steady = {"value": pts * WORK["total_steps"] / (sms * 1e-3), "ms": sms,
+                          "steps": WORK["total_steps"], "launches": sl}
+        if dist is not None:
+            t = torch.tensor([ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        res[name] = dict(ms=ms, launches=launches, clocks=clocks, steady=steady)
+
+    tsteps = args.steps * STEPS_PER_BENCH_STEP
+    v32 = world * pts * tsteps / (res["fp32"]["ms"] * 1e-3)
+    v64 = world * pts * tsteps / (res["fp64"]["ms"] * 1e-3)
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        peak, peak_src = 6650.0, "fallback"
+    # algorithmic bytes: P = 4 full-field read+write passes per time step for
+    # 2D with the gauge, complex64 (8 B): 2*4*8 = 64 B per grid point and step
+    alg_bytes_per_step = 2 * 4 * 8 * pts
+    per_time_step_s = res["fp32"]["ms"] * 1e-3 / tsteps
+    achieved = alg_bytes_per_step / per_time_step_s / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get("cfg2_fp32_pass_bytes_per_launch")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic,
+                "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)" if peak_src ==
+                "measured" else "fallback 6.65 TB/s",
+                "note": "achieved = 16 MiB algorithmic bytes per pass launch (read+write of "
+                        "the complex64 field) / mean pass duration (4 passes per time step)"}
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = cpu_oracle_rate(psi0)
+    e2e = None if args.quick else e2e_leg(G, torch, psi0, dev)
+    acc = accuracy_leg(G, psi0, dev)
+    line = {
+        "metric": METRIC, "value": v32, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": res["fp32"]["ms"] / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded; FP64 imaginary-time relaxed state x smoothed random phase)",
+        "config": {"workload": WORKLOAD_NAME, "grid": WORK["n"], "form": "fused complex64, "
+                   "FP64 operator phases rounded, FP64 reductions",
+                   "step": "%d split-operator time steps (one x/y gauge-order cycle)"
+                           % STEPS_PER_BENCH_STEP,
+                   "l2": "flushed before every timed step (256 MiB write)",
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "plain_fp64": {"value": v64, "ms_per_step": res["fp64"]["ms"] / args.steps,
+                       "fused_fp32_over_plain_fp64": v32 / v64},
+        "steady_state": {"fp32": res["fp32"]["steady"], "fp64": res["fp64"]["steady"],
+                         "note": "one gpue_evolve call of 20000 steps (the configuration's "
+                                 "length), graph-replayed, no L2 flush"},
+        "accuracy": acc,
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+        "clocks": res["fp32"]["clocks"],
+        "gpu_launches": res["fp32"]["launches"],
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

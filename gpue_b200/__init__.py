@@ -1,0 +1,235 @@
+"""gpue_b200: B200-native split-operator Gross-Pitaevskii step (GPUE's evolve()).
+
+The product is the C-ABI shared library ``libgpue_b200.so`` built from
+``gpue_b200/csrc`` (declared in ``include/gpue_b200.h``).  This module is a thin
+ctypes mirror of that ABI for Python callers (tests, benchmarks).  Importing
+it loads the library and raises if it has not been built: there is no
+fallback implementation.
+"""
+
+import ctypes as C
+import os
+
+import numpy as np
+
+__all__ = ["lib", "Params", "EvolveOpts", "EvolveResult", "Solver", "GpueError",
+           "PREC_FP64", "PREC_FP32", "C128", "C64", "MEM_HOST", "MEM_DEVICE",
+           "GAUGE_ROTATION", "GAUGE_CONSTANT", "supported_length", "default_params"]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgpue_b200.so")
+
+PREC_FP64, PREC_FP32 = 0, 1
+MEM_HOST, MEM_DEVICE = 0, 1
+C128, C64 = 0, 1
+GAUGE_ROTATION, GAUGE_CONSTANT = 0, 1
+
+STATUS = {0: "GPUE_OK", 1: "GPUE_ERR_INVALID_ARG", 2: "GPUE_ERR_UNSUPPORTED",
+          3: "GPUE_ERR_CUDA", 4: "GPUE_ERR_OUT_OF_MEMORY", 5: "GPUE_ERR_AST",
+          6: "GPUE_ERR_STATE", 7: "GPUE_ERR_TIMEOUT"}
+
+
+class GpueError(RuntimeError):
+    def __init__(self, status, msg=""):
+        self.status = status
+        super().__init__("%s%s" % (STATUS.get(status, str(status)), (": " + msg) if msg else ""))
+
+
+class Params(C.Structure):
+    _fields_ = [("dimnum", C.c_int32), ("xDim", C.c_int32), ("yDim", C.c_int32),
+                ("zDim", C.c_int32), ("xMax", C.c_double), ("yMax", C.c_double),
+                ("zMax", C.c_double), ("hbar", C.c_double), ("mass", C.c_double),
+                ("omegaX", C.c_double), ("omegaY", C.c_double), ("omegaZ", C.c_double),
+                ("gammaY", C.c_double), ("x0_shift", C.c_double), ("y0_shift", C.c_double),
+                ("z0_shift", C.c_double), ("omega", C.c_double), ("interaction", C.c_double),
+                ("gDenConst", C.c_double), ("gdt", C.c_double), ("dt", C.c_double),
+                ("gpe", C.c_int32), ("corotating", C.c_int32), ("gauge", C.c_int32),
+                ("ramp", C.c_int32), ("ramp_type", C.c_int32), ("precision", C.c_int32),
+                ("device", C.c_int32), ("reserved", C.c_int32 * 8)]
+
+
+class EvolveOpts(C.Structure):
+    _fields_ = [("energy_calc_steps", C.c_int32), ("energy_calc_threshold", C.c_double),
+                ("threshold_abs", C.c_int32), ("polish_steps", C.c_int32),
+                ("graph_chunk", C.c_int32), ("no_sync", C.c_int32),
+                ("step_offset", C.c_int32), ("reserved", C.c_int32 * 5)]
+
+
+class EvolveResult(C.Structure):
+    _fields_ = [("steps_done", C.c_int32), ("early_stop", C.c_int32),
+                ("n_energies", C.c_int32), ("reserved0", C.c_int32), ("energy", C.c_double),
+                ("norm", C.c_double), ("device_ms", C.c_double),
+                ("kernel_launches", C.c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("reserved")}
+
+
+_lib = None
+
+
+def lib():
+    """The loaded libgpue_b200.so (raises if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libgpue_b200.so is not built; run `make -C gpue_b200` "
+                              "(or __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        vp, i32 = C.c_void_p, C.c_int32
+        L.gpue_abi_version.restype = C.c_int
+        L.gpue_default_params.argtypes = [C.POINTER(Params)]
+        L.gpue_ctx_create.argtypes = [C.POINTER(Params), C.POINTER(vp)]
+        L.gpue_ctx_destroy.argtypes = [vp]
+        L.gpue_last_error.argtypes = [vp]
+        L.gpue_last_error.restype = C.c_char_p
+        L.gpue_supported_length.argtypes = [i32, i32]
+        L.gpue_set_operators.argtypes = [vp, i32]
+        L.gpue_set_wfc.argtypes = [vp, vp, i32, i32]
+        L.gpue_get_wfc.argtypes = [vp, vp, i32, i32]
+        L.gpue_evolve.argtypes = [vp, i32, i32, C.POINTER(EvolveOpts), C.POINTER(EvolveResult)]
+        L.gpue_energy.argtypes = [vp, C.POINTER(C.c_double)]
+        L.gpue_norm.argtypes = [vp, C.POINTER(C.c_double)]
+        L.gpue_ctx_stream.argtypes = [vp, C.POINTER(vp)]
+        L.gpue_ctx_wfc_device.argtypes = [vp, C.POINTER(vp), C.POINTER(i32)]
+        for name in ("gpue_default_params", "gpue_ctx_create", "gpue_ctx_destroy",
+                     "gpue_set_operators", "gpue_set_wfc", "gpue_get_wfc", "gpue_evolve",
+                     "gpue_energy", "gpue_norm", "gpue_ctx_stream", "gpue_ctx_wfc_device"):
+            getattr(L, name).restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def supported_length(n, precision=PREC_FP64):
+    return bool(lib().gpue_supported_length(precision, n))
+
+
+def default_params():
+    p = Params()
+    _check(lib().gpue_default_params(C.byref(p)))
+    return p
+
+
+def _check(st, ctx=None):
+    if st != 0:
+        msg = lib().gpue_last_error(ctx).decode() if ctx else ""
+        raise GpueError(st, msg)
+
+
+def make_params(dim, n, box, hbar=1.0, mass=1.0, wx=1.0, wy=1.0, wz=1.0, gamma=1.0, g=0.0,
+                gpe=True, omega=0.0, gauge=False, gdt=1e-4, dt=1e-4, precision=PREC_FP64,
+                ramp=False, ramp_type=1, device=0, shifts=(0.0, 0.0, 0.0)):
+    """Params for a square/cubic run with gN = g (interaction = g, gDenConst = 1)."""
+    p = Params()
+    p.dimnum = dim
+    p.xDim = p.yDim = n
+    p.zDim = n if dim == 3 else 1
+    p.xMax = p.yMax = p.zMax = box
+    p.hbar, p.mass = hbar, mass
+    p.omegaX, p.omegaY, p.omegaZ, p.gammaY = wx, wy, wz, gamma
+    p.x0_shift, p.y0_shift, p.z0_shift = shifts
+    p.omega = omega
+    p.interaction, p.gDenConst = g, 1.0
+    p.gdt, p.dt = gdt, dt
+    p.gpe = 1 if gpe else 0
+    p.corotating = 1 if gauge else 0
+    p.gauge = GAUGE_ROTATION
+    p.ramp, p.ramp_type = (1 if ramp else 0), ramp_type
+    p.precision = precision
+    p.device = device
+    return p
+
+
+class Solver:
+    """One context of the C ABI: resident wavefunction plus operators."""
+
+    def __init__(self, params):
+        self.params = params
+        h = C.c_void_p()
+        _check(lib().gpue_ctx_create(C.byref(params), C.byref(h)))
+        self._h = h
+        d = params.dimnum
+        n = params.xDim
+        self.shape = (n, n, n) if d == 3 else (n, n)
+        self.precision = params.precision
+
+    def close(self):
+        if self._h:
+            lib().gpue_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _ck(self, st):
+        _check(st, self._h)
+
+    def set_operators(self, ev_type):
+        self._ck(lib().gpue_set_operators(self._h, ev_type))
+
+    def set_wfc(self, psi):
+        a = np.ascontiguousarray(psi)
+        if a.dtype == np.complex128:
+            dt = C128
+        elif a.dtype == np.complex64:
+            dt = C64
+        else:
+            raise TypeError("psi must be complex64 or complex128")
+        if a.size != int(np.prod(self.shape)):
+            raise ValueError("psi has %d points, grid has %d" % (a.size, np.prod(self.shape)))
+        self._ck(lib().gpue_set_wfc(self._h, a.ctypes.data_as(C.c_void_p), MEM_HOST, dt))
+
+    def get_wfc(self, dtype=np.complex128):
+        out = np.empty(self.shape, dtype=dtype)
+        dt = C128 if out.dtype == np.complex128 else C64
+        self._ck(lib().gpue_get_wfc(self._h, out.ctypes.data_as(C.c_void_p), MEM_HOST, dt))
+        return out
+
+    def set_wfc_device(self, ptr, dtype):
+        self._ck(lib().gpue_set_wfc(self._h, C.c_void_p(ptr), MEM_DEVICE, dtype))
+
+    def get_wfc_device(self, ptr, dtype):
+        self._ck(lib().gpue_get_wfc(self._h, C.c_void_p(ptr), MEM_DEVICE, dtype))
+
+    def evolve(self, nsteps, gstate, energy_every=0, threshold=-1.0, threshold_abs=False,
+               polish_steps=0, graph_chunk=0, no_sync=False, step_offset=0):
+        o = EvolveOpts()
+        o.no_sync = 1 if no_sync else 0
+        o.step_offset = step_offset
+        o.energy_calc_steps = energy_every
+        o.energy_calc_threshold = threshold
+        o.threshold_abs = 1 if threshold_abs else 0
+        o.polish_steps = polish_steps
+        o.graph_chunk = graph_chunk
+        r = EvolveResult()
+        self._ck(lib().gpue_evolve(self._h, nsteps, gstate, C.byref(o), C.byref(r)))
+        return r.as_dict()
+
+    def energy(self):
+        e = C.c_double()
+        self._ck(lib().gpue_energy(self._h, C.byref(e)))
+        return e.value
+
+    def norm(self):
+        e = C.c_double()
+        self._ck(lib().gpue_norm(self._h, C.byref(e)))
+        return e.value
+
+    def stream(self):
+        s = C.c_void_p()
+        self._ck(lib().gpue_ctx_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+    def wfc_device(self):
+        p, d = C.c_void_p(), C.c_int32()
+        self._ck(lib().gpue_ctx_wfc_device(self._h, C.byref(p), C.byref(d)))
+        return p.value, d.value

@@ -1,0 +1,292 @@
+// fft_core.cuh -- the line FFT engine used by every pass kernel.
+//
+// A "line" is one 1D transform of length N along one axis of the field.  P
+// threads cooperate on a line; each holds E = N/P complex values in registers.
+// The transform is a Stockham autosort FFT (Govindaraju et al., "High
+// performance discrete Fourier transforms on graphics processors", SC'08)
+// with a palindromic radix sequence (RA, RA) or (RA, RB, RA):
+//
+//   stage s, radix R, Ns = product of earlier radices, j = t + P*q:
+//     inputs   x[j + r*N/R]             (r < R, read from registers/smem)
+//     twiddle  W_{Ns R}^{(j mod Ns) r}  (from a per-N table W_N^k)
+//     R-point DFT in registers
+//     outputs  y[(j/Ns)*Ns*R + (j mod Ns) + r*Ns]
+//
+// Stage 0 reads straight from the registers loaded from HBM, the last stage
+// leaves its outputs in registers, and the middle exchanges go through shared
+// memory.  Because the sequence is palindromic, the register layout before and
+// after a transform is the same ("layout D": register e = q*RA + r holds
+// element t + P*q + r*N/RA), so forward and inverse transforms and pointwise
+// phase multiplies chain inside one kernel without extra data movement, and
+// global loads/stores in layout D are coalesced across threads.
+//
+// The unnormalised DFT convention is cuFFT's (forward exp(-2 pi i jk/N),
+// inverse exp(+2 pi i jk/N)), which is what GPUE's evolve() uses.
+
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <utility>
+
+#include "twiddles.h"
+
+namespace gpue {
+
+template <typename T>
+struct alignas(2 * sizeof(T)) cx {
+    T x, y;
+};
+
+template <typename T>
+__device__ __forceinline__ cx<T> operator+(cx<T> a, cx<T> b) { return {a.x + b.x, a.y + b.y}; }
+template <typename T>
+__device__ __forceinline__ cx<T> operator-(cx<T> a, cx<T> b) { return {a.x - b.x, a.y - b.y}; }
+template <typename T>
+__device__ __forceinline__ cx<T> cmul(cx<T> a, cx<T> b) {
+    return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+template <typename T>
+__device__ __forceinline__ cx<T> cscale(cx<T> a, T s) { return {a.x * s, a.y * s}; }
+template <typename T>
+__device__ __forceinline__ cx<T> cconj(cx<T> a) { return {a.x, -a.y}; }
+// multiply by -i (forward) or +i (inverse)
+template <bool INV, typename T>
+__device__ __forceinline__ cx<T> mul_mi(cx<T> a) {
+    if constexpr (INV) return {-a.y, a.x};
+    else return {a.y, -a.x};
+}
+
+// a * W_R^m with W_R = exp(-2 pi i / R) (forward) or its conjugate (inverse);
+// exact shortcuts for the multiples of pi/2 and pi/4.
+template <int R, int M, bool INV, typename T>
+__device__ __forceinline__ cx<T> tw_const(cx<T> a) {
+    constexpr int m = ((M % R) + R) % R;
+    if constexpr (m == 0) {
+        return a;
+    } else if constexpr (2 * m == R) {
+        return {-a.x, -a.y};
+    } else if constexpr (4 * m == R) {
+        return mul_mi<INV>(a);
+    } else if constexpr (4 * m == 3 * R) {
+        return mul_mi<!INV>(a);
+    } else if constexpr (8 * m == R || 8 * m == 3 * R || 8 * m == 5 * R || 8 * m == 7 * R) {
+        constexpr T h = (T)0.70710678118654752440;
+        constexpr double c = tw_cos(R, m);
+        constexpr double s = tw_sin(R, m);
+        // (c - i s) for forward, (c + i s) inverse; |c| = |s| = h
+        constexpr T cs = c > 0 ? h : -h;
+        constexpr T ss = INV ? (s > 0 ? h : -h) : (s > 0 ? -h : h);
+        return {cs * a.x - ss * a.y, cs * a.y + ss * a.x};
+    } else {
+        constexpr T c = (T)tw_cos(R, m);
+        constexpr T s = INV ? (T)tw_sin(R, m) : (T)-tw_sin(R, m);
+        return {c * a.x - s * a.y, c * a.y + s * a.x};
+    }
+}
+
+// ---------------------------------------------------------- small DFTs --
+// In-place R-point DFT of v[0..R-1] in registers, natural-order output.
+
+template <int R, bool INV, typename T>
+struct SmallDFT;
+
+template <bool INV, typename T>
+struct SmallDFT<2, INV, T> {
+    static __device__ __forceinline__ void run(cx<T>* v) {
+        cx<T> a = v[0], b = v[1];
+        v[0] = a + b;
+        v[1] = a - b;
+    }
+};
+
+template <bool INV, typename T>
+struct SmallDFT<3, INV, T> {
+    static __device__ __forceinline__ void run(cx<T>* v) {
+        constexpr T c1 = (T)-0.5;
+        constexpr T s1 = INV ? (T)tw_sin(3, 1) : (T)-tw_sin(3, 1);
+        cx<T> t1 = v[1] + v[2];
+        cx<T> t2 = v[1] - v[2];
+        cx<T> a = {v[0].x + c1 * t1.x, v[0].y + c1 * t1.y};
+        cx<T> b = {-s1 * t2.y, s1 * t2.x};  // i*s1*t2
+        v[0] = v[0] + t1;
+        v[1] = a + b;
+        v[2] = a - b;
+    }
+};
+
+template <bool INV, typename T>
+struct SmallDFT<4, INV, T> {
+    static __device__ __forceinline__ void run(cx<T>* v) {
+        cx<T> s02 = v[0] + v[2], d02 = v[0] - v[2];
+        cx<T> s13 = v[1] + v[3], d13 = mul_mi<INV>(v[1] - v[3]);
+        v[0] = s02 + s13;
+        v[1] = d02 + d13;
+        v[2] = s02 - s13;
+        v[3] = d02 - d13;
+    }
+};
+
+template <bool INV, typename T>
+struct SmallDFT<5, INV, T> {
+    static __device__ __forceinline__ void run(cx<T>* v) {
+        constexpr T c1 = (T)tw_cos(5, 1), c2 = (T)tw_cos(5, 2);
+        constexpr T s1 = INV ? (T)tw_sin(5, 1) : (T)-tw_sin(5, 1);
+        constexpr T s2 = INV ? (T)tw_sin(5, 2) : (T)-tw_sin(5, 2);
+        cx<T> a1 = v[1] + v[4], b1 = v[1] - v[4];
+        cx<T> a2 = v[2] + v[3], b2 = v[2] - v[3];
+        cx<T> r1 = {v[0].x + c1 * a1.x + c2 * a2.x, v[0].y + c1 * a1.y + c2 * a2.y};
+        cx<T> r2 = {v[0].x + c2 * a1.x + c1 * a2.x, v[0].y + c2 * a1.y + c1 * a2.y};
+        // i*(s1 b1 + s2 b2) and i*(s2 b1 - s1 b2)
+        cx<T> i1 = {-(s1 * b1.y + s2 * b2.y), s1 * b1.x + s2 * b2.x};
+        cx<T> i2 = {-(s2 * b1.y - s1 * b2.y), s2 * b1.x - s1 * b2.x};
+        v[0] = v[0] + a1 + a2;
+        v[1] = r1 + i1;
+        v[4] = r1 - i1;
+        v[2] = r2 + i2;
+        v[3] = r2 - i2;
+    }
+};
+
+// Composite R = A*B (A the smallest prime-power factor handled directly):
+// B DFTs of length A on stride-B subsequences, twiddles W_R^{b k1}, then A
+// DFTs of length B; X[k1 + A*k2].
+template <int R>
+struct Split {
+    static constexpr int A = (R % 4 == 0 && R != 8 && R != 4) ? 4
+                             : (R % 2 == 0) ? 2
+                             : (R % 3 == 0) ? 3
+                                            : 5;
+    static constexpr int B = R / A;
+};
+
+template <int R, bool INV, typename T>
+struct SmallDFT {
+    static constexpr int A = Split<R>::A;
+    static constexpr int B = Split<R>::B;
+    template <int b, int k1>
+    static __device__ __forceinline__ void tw_one(cx<T> (&y)[B][A]) {
+        y[b][k1] = tw_const<R, b * k1, INV>(y[b][k1]);
+    }
+    static __device__ __forceinline__ void run(cx<T>* v) {
+        cx<T> y[B][A];
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+#pragma unroll
+            for (int a = 0; a < A; ++a) y[b][a] = v[b + B * a];
+            SmallDFT<A, INV, T>::run(y[b]);
+        }
+        twiddle_all(y, std::make_integer_sequence<int, B * A>{});
+        cx<T> z[B];
+#pragma unroll
+        for (int k1 = 0; k1 < A; ++k1) {
+#pragma unroll
+            for (int b = 0; b < B; ++b) z[b] = y[b][k1];
+            SmallDFT<B, INV, T>::run(z);
+#pragma unroll
+            for (int k2 = 0; k2 < B; ++k2) v[k1 + A * k2] = z[k2];
+        }
+    }
+    template <int... I>
+    static __device__ __forceinline__ void twiddle_all(cx<T> (&y)[B][A],
+                                                       std::integer_sequence<int, I...>) {
+        (tw_one<I / A, I % A>(y), ...);
+    }
+};
+
+// ------------------------------------------------------------ line FFT --
+
+__device__ __forceinline__ int smem_phys(int i) { return i + (i >> 5); }
+
+template <typename T, int N_, int RA, int RB, int P_>
+struct LineFFT {
+    static constexpr int N = N_;
+    static constexpr int P = P_;
+    static constexpr int NS = RB ? 3 : 2;
+    static constexpr int E = N / P;
+    static_assert(NS == 2 ? N == RA * RA : N == RA * RB * RA, "palindromic radix plan");
+    static_assert((N / RA) % P == 0, "threads must divide the butterflies of the outer stages");
+    static_assert(NS == 2 || (N / RB) % P == 0, "threads must divide the middle stage");
+    // smem line stride (elements of T per re/im array): one pad per 32, plus a
+    // bank offset so lines that share a warp land on different banks
+    static constexpr int LS = N + N / 32 + 8;
+
+    __host__ __device__ static constexpr int radix(int s) { return (NS == 3 && s == 1) ? RB : RA; }
+    __host__ __device__ static constexpr int ns_before(int s) { return s == 0 ? 1 : s == 1 ? RA : RA * RB; }
+
+    // element index held by register e in layout D
+    static __device__ __forceinline__ int index(int t, int e) {
+        return t + P * (e / RA) + (e % RA) * (N / RA);
+    }
+
+    template <int S, bool INV>
+    static __device__ __forceinline__ void compute(cx<T> (&v)[E], int t,
+                                                   const cx<T>* __restrict__ tw) {
+        constexpr int R = radix(S);
+        constexpr int Ns = ns_before(S);
+        constexpr int G = N / (R * P);
+#pragma unroll
+        for (int q = 0; q < G; ++q) {
+            if constexpr (S > 0) {
+                const int j = t + P * q;
+                const int jm = j % Ns;
+                constexpr int step = N / (Ns * R);
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    cx<T> w = tw[jm * r * step];
+                    if constexpr (INV) w.y = -w.y;
+                    v[q * R + r] = cmul(v[q * R + r], w);
+                }
+            }
+            SmallDFT<R, INV, T>::run(&v[q * R]);
+        }
+    }
+
+    // Write stage S's outputs to smem, sync, read stage S+1's inputs, sync.
+    template <int S, typename Sync>
+    static __device__ __forceinline__ void exchange(cx<T> (&v)[E], int t, T* sre, T* sim,
+                                                    Sync sync) {
+        constexpr int R = radix(S);
+        constexpr int Ns = ns_before(S);
+        constexpr int G = N / (R * P);
+#pragma unroll
+        for (int q = 0; q < G; ++q) {
+            const int j = t + P * q;
+            const int base = (j / Ns) * Ns * R + (j % Ns);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int p = smem_phys(base + r * Ns);
+                sre[p] = v[q * R + r].x;
+                sim[p] = v[q * R + r].y;
+            }
+        }
+        sync();
+        constexpr int R2 = radix(S + 1);
+        constexpr int G2 = N / (R2 * P);
+#pragma unroll
+        for (int q = 0; q < G2; ++q) {
+            const int j = t + P * q;
+#pragma unroll
+            for (int r = 0; r < R2; ++r) {
+                const int p = smem_phys(j + r * (N / R2));
+                v[q * R2 + r] = cx<T>{sre[p], sim[p]};
+            }
+        }
+        sync();
+    }
+
+    template <bool INV, typename Sync>
+    static __device__ __forceinline__ void run(cx<T> (&v)[E], int t, T* sre, T* sim,
+                                               const cx<T>* __restrict__ tw, Sync sync) {
+        compute<0, INV>(v, t, tw);
+        exchange<0>(v, t, sre, sim, sync);
+        compute<1, INV>(v, t, tw);
+        if constexpr (NS == 3) {
+            exchange<1>(v, t, sre, sim, sync);
+            compute<2, INV>(v, t, tw);
+        }
+    }
+};
+
+}  // namespace gpue

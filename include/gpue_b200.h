@@ -1,0 +1,154 @@
+/*
+ * gpue_b200.h -- C ABI of the B200-native split-operator Gross-Pitaevskii step.
+ *
+ * This is the drop-in boundary for GPUE's time stepper.  Plain C types only
+ * (pointers, sizes, PODs); every call returns a status code and never exits.
+ * The entry points replace these GPUE interfaces (GPUE-group/GPUE):
+ *
+ *   gpue_ctx_create      init() + generate_fields()  src/init.cu:40-356,
+ *                        src/operators.cu:722-992 (grids, K, A, V, operator
+ *                        tables), with the Grid keys of include/ds.h:86-196
+ *                        passed as a gpue_params POD
+ *   gpue_set_operators   set_variables(par, ev_type)  src/init.cu:358-497
+ *   gpue_set_wfc /
+ *   gpue_get_wfc         the "wfc"/"wfc_gpu" Grid entries (src/init.cu:525-539,
+ *                        src/evolution.cu:430, 906-907)
+ *   gpue_evolve          evolve(par, numSteps, gstate, buffer)
+ *                        include/evolution.h:54-57, src/evolution.cu:260-908
+ *   gpue_energy          energy_calc(par, wfc)  src/split_op.cu:208-375
+ *   gpue_last_error      cudaHandleError/cudaCheckError/cufftHandleError
+ *                        (src/split_op.cu:40-59) report-and-exit replaced by
+ *                        status codes plus a message
+ *
+ * Units follow the caller: GPUE itself uses SI with the Rb-87 mass; hbar = m = 1
+ * is equally valid.  Grids are square (2D) or cubic (3D), x fastest in memory
+ * (index x + xDim*(y + yDim*z)), x_i = -xMax + i*dx with dx = xMax/(xDim/2),
+ * as GPUE's generate_p_space lays them out.
+ *
+ * Threading: a context owns one CUDA stream; calls on one context must not
+ * overlap; distinct contexts may be used from distinct threads.
+ */
+#ifndef GPUE_B200_H
+#define GPUE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GPUE_B200_ABI_VERSION 1
+
+typedef enum gpue_status {
+    GPUE_OK = 0,
+    GPUE_ERR_INVALID_ARG = 1,   /* bad size, pointer or flag */
+    GPUE_ERR_UNSUPPORTED = 2,   /* grid length without a compiled FFT plan, ... */
+    GPUE_ERR_CUDA = 3,          /* a CUDA runtime call failed (message in last_error) */
+    GPUE_ERR_OUT_OF_MEMORY = 4, /* device allocation failed or budget exceeded */
+    GPUE_ERR_AST = 5,           /* equation string did not parse */
+    GPUE_ERR_STATE = 6,         /* call out of order (e.g. no wavefunction set) */
+    GPUE_ERR_TIMEOUT = 7        /* a bounded device wait gave up */
+} gpue_status;
+
+enum { GPUE_PREC_FP64 = 0, GPUE_PREC_FP32 = 1 };
+enum { GPUE_MEM_HOST = 0, GPUE_MEM_DEVICE = 1 };
+enum { GPUE_C128 = 0, GPUE_C64 = 1 };
+/* gauge field presets (GPUE's -A flag, src/ds.cu:300-331) */
+enum { GPUE_GAUGE_ROTATION = 0, GPUE_GAUGE_CONSTANT = 1 };
+
+typedef struct gpue_ctx gpue_ctx;
+
+/* The Grid keys evolve() and its callers read (src/evolution.cu:266-332). */
+typedef struct gpue_params {
+    int32_t dimnum;            /* 2 or 3 ("dimnum", -c) */
+    int32_t xDim, yDim, zDim;  /* equal; zDim = 1 in 2D (-x -y -z) */
+    double xMax, yMax, zMax;   /* half box widths ("xMax", -b) */
+    double hbar, mass;         /* HBAR (include/constants.h:20), "mass" */
+    double omegaX, omegaY, omegaZ, gammaY; /* trap (-X -Y -Z -G) */
+    double x0_shift, y0_shift, z0_shift;   /* trap centre shifts (-U -V -Q) */
+    double omega;              /* rotation rate scaling the gauge field (-w) */
+    double interaction;        /* -i */
+    double gDenConst;          /* nonlinear prefactor; gN = interaction*gDenConst */
+    double gdt, dt;            /* imaginary / real time steps (-T -t) */
+    int32_t gpe;               /* nonlinear term on (-s) */
+    int32_t corotating;        /* gauge passes and L energy term on (-l) */
+    int32_t gauge;             /* GPUE_GAUGE_* (-A) */
+    int32_t ramp, ramp_type;   /* gauge ramp in imaginary time (-R) */
+    int32_t precision;         /* GPUE_PREC_FP64 (plain) or GPUE_PREC_FP32 (fused) */
+    int32_t device;            /* CUDA device ordinal (-C) */
+    int32_t reserved[8];       /* zero */
+} gpue_params;
+
+typedef struct gpue_evolve_opts {
+    int32_t energy_calc_steps;     /* energy every k steps (0: never), "-E thr k" */
+    double energy_calc_threshold;  /* early-stop threshold (imaginary time) */
+    int32_t threshold_abs;         /* 0: |E_old-E| < thr*E_old as GPUE, 1: |E_old-E| < thr */
+    int32_t polish_steps;          /* FP64 steps after an FP32 imaginary-time run */
+    int32_t graph_chunk;           /* steps per captured CUDA graph; 0 = automatic */
+    int32_t no_sync;               /* 1: return once the steps are enqueued on the
+                                      context stream (no energy checks allowed);
+                                      result then holds steps_done and launches only */
+    int32_t step_offset;           /* first step index (GPUE starts every evolve() at
+                                      0); lets a run continue in slices with the same
+                                      time = Dt*i and gauge order i%2 */
+    int32_t reserved[5];
+} gpue_evolve_opts;
+
+typedef struct gpue_evolve_result {
+    int32_t steps_done;
+    int32_t early_stop;
+    int32_t n_energies;
+    int32_t reserved0;
+    double energy;     /* last energy computed, NaN if none */
+    double norm;       /* sum |psi|^2 dV of the final state */
+    double device_ms;  /* device time of the step loop (CUDA events) */
+    int64_t kernel_launches; /* kernels enqueued by this call */
+} gpue_evolve_result;
+
+int gpue_abi_version(void);
+
+/* Defaults of GPUE's parseArgs (src/parser.cu:14-67) in the given units. */
+gpue_status gpue_default_params(gpue_params* p);
+
+/* init(): validates sizes, allocates the device state and builds the
+ * per-axis operator tables.  Fails with GPUE_ERR_UNSUPPORTED for lengths with
+ * no compiled FFT plan (see gpue_supported_length). */
+gpue_status gpue_ctx_create(const gpue_params* p, gpue_ctx** out);
+gpue_status gpue_ctx_destroy(gpue_ctx* ctx);
+const char* gpue_last_error(const gpue_ctx* ctx);
+
+/* 1 if an FFT plan is compiled for this line length in this precision. */
+int gpue_supported_length(int32_t precision, int32_t n);
+
+/* set_variables(): prepares the imaginary (0) or real (1) time operators. */
+gpue_status gpue_set_operators(gpue_ctx* ctx, int32_t ev_type);
+
+/* Wavefunction in/out, x fastest; mem = GPUE_MEM_*, dtype = GPUE_C128/C64.
+ * Host pointers may be pageable or pinned; device pointers must be on the
+ * context's device. */
+gpue_status gpue_set_wfc(gpue_ctx* ctx, const void* psi, int32_t mem, int32_t dtype);
+gpue_status gpue_get_wfc(gpue_ctx* ctx, void* psi, int32_t mem, int32_t dtype);
+
+/* evolve(): nsteps split-operator steps, imaginary (gstate 0) or real (1)
+ * time.  Step numbering restarts at 0 on every call as in GPUE (time = Dt*i,
+ * gauge order alternates with i%2).  opts and result may be NULL. */
+gpue_status gpue_evolve(gpue_ctx* ctx, int32_t nsteps, int32_t gstate,
+                        const gpue_evolve_opts* opts, gpue_evolve_result* result);
+
+/* energy_calc(): <psi|H|psi> dV of the current state (no division by the norm). */
+gpue_status gpue_energy(gpue_ctx* ctx, double* energy);
+
+/* sum |psi|^2 dV of the current state. */
+gpue_status gpue_norm(gpue_ctx* ctx, double* norm);
+
+/* The context's cudaStream_t (as void*) for callers that time or order work. */
+gpue_status gpue_ctx_stream(gpue_ctx* ctx, void** stream);
+
+/* Device pointer of the resident wavefunction and its dtype (GPUE_C128/C64). */
+gpue_status gpue_ctx_wfc_device(gpue_ctx* ctx, void** psi, int32_t* dtype);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPUE_B200_H */

@@ -1,0 +1,160 @@
+// ref_harness.cu -- TEST INFRASTRUCTURE ONLY.
+//
+// Drives GPUE's own CUDA build (its parseArgs, init, set_variables, evolve and
+// energy_calc, compiled unmodified from the reference sources) on a seeded
+// initial wavefunction, and writes the final device wavefunction and energy
+// in binary/text so the tests can pin the CPU oracle and the CUDA product to
+// the reference itself.
+//
+// GPUE works in SI units with hbar = 1.05457148e-34 (include/constants.h:20)
+// and forces the Rb-87 mass (src/init.cu:98).  The dimensionless problem
+// (hbar = m = 1) maps onto it exactly with a time unit of 1 s and a length
+// unit L = sqrt(hbar/m):  x_SI = x L,  p_SI = p / L,  t and omega unchanged,
+// E_SI = hbar E,  psi_SI = psi / L^(d/2),  gN_SI = g hbar L^d.  The gauge
+// field A = omega*(-y wx, x wy) and the +m|A|^2/2 term in V map the same way.
+//
+// Usage (key=value):
+//   gpue_ref_harness dim=2 n=64 box=10 wx=1 wy=1 wz=1 gamma=1 g=100 gpe=1
+//       omega=0 gauge=0 gdt=1e-4 dt=1e-4 gsteps=100 esteps=0 energy_every=0
+//       psi0=in.bin out=prefix data=/tmp/dir
+// Writes prefix_imag.bin / prefix_real.bin (complex128, x fastest, hbar=m=1
+// units) and prefix_imag.txt / prefix_real.txt ("energy <E>" and
+// "last_check_energy <E>", plus "evolve_s <seconds>" of the evolve() call).
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "constants.h"
+#include "ds.h"
+#include "evolution.h"
+#include "init.h"
+#include "parser.h"
+#include "split_op.h"
+
+namespace {
+
+std::map<std::string, std::string> g_kv;
+
+std::string get(const char* k, const char* def) {
+    auto it = g_kv.find(k);
+    return it == g_kv.end() ? std::string(def) : it->second;
+}
+double getd(const char* k, double def) {
+    auto it = g_kv.find(k);
+    return it == g_kv.end() ? def : atof(it->second.c_str());
+}
+int geti(const char* k, int def) {
+    auto it = g_kv.find(k);
+    return it == g_kv.end() ? def : atoi(it->second.c_str());
+}
+std::string fmt(double v) {
+    char b[64];
+    snprintf(b, sizeof b, "%.17g", v);
+    return b;
+}
+
+void dump(Grid& par, const std::string& path, int gsize, double L, int dim, double secs) {
+    double2* dev = par.cufftDoubleComplexval("wfc_gpu");
+    std::vector<double2> h(gsize);
+    cudaMemcpy(h.data(), dev, sizeof(double2) * gsize, cudaMemcpyDeviceToHost);
+    double s = std::pow(L, 0.5 * dim);
+    for (auto& v : h) { v.x *= s; v.y *= s; }
+    FILE* f = fopen((path + ".bin").c_str(), "wb");
+    fwrite(h.data(), sizeof(double2), gsize, f);
+    fclose(f);
+    double e = energy_calc(par, dev) / HBAR;
+    double last = par.dval("energy") / HBAR;
+    FILE* t = fopen((path + ".txt").c_str(), "w");
+    fprintf(t, "energy %.17g\nlast_check_energy %.17g\nevolve_s %.6f\n", e, last, secs);
+    fclose(t);
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    for (int i = 1; i < argc; ++i) {
+        std::string a = argv[i];
+        size_t eq = a.find('=');
+        if (eq != std::string::npos) g_kv[a.substr(0, eq)] = a.substr(eq + 1);
+    }
+    const int dim = geti("dim", 2);
+    const int n = geti("n", 64);
+    const int gsteps = geti("gsteps", 0), esteps = geti("esteps", 0);
+    const double mass = 1.4431607e-25;  // the mass init() stores
+    const double L = std::sqrt(HBAR / mass);
+    const std::string data = get("data", "/tmp/gpue_ref_data");
+
+    std::vector<std::string> a = {"gpue", "-c", std::to_string(dim),
+                                  "-x", std::to_string(n), "-y", std::to_string(n)};
+    if (dim == 3) { a.push_back("-z"); a.push_back(std::to_string(n)); }
+    // -c 3 resets box_size, so -b comes after it
+    for (auto s : {std::string("-b"), fmt(getd("box", 10) * L),
+                   std::string("-X"), fmt(getd("wx", 1)), std::string("-Y"), fmt(getd("wy", 1)),
+                   std::string("-Z"), fmt(getd("wz", 1)), std::string("-G"), fmt(getd("gamma", 1)),
+                   std::string("-T"), fmt(getd("gdt", 1e-4)), std::string("-t"), fmt(getd("dt", 1e-4)),
+                   std::string("-g"), std::to_string(gsteps), std::string("-e"), std::to_string(esteps),
+                   std::string("-p"), std::to_string((gsteps > esteps ? gsteps : esteps) + 1),
+                   std::string("-f"), std::string("-d"), data})
+        a.push_back(s);
+    if (geti("gpe", 1)) a.push_back("-s");
+    if (geti("gauge", 0)) {
+        a.push_back("-l");
+        a.push_back("-w");
+        a.push_back(fmt(getd("omega", 0)));
+    }
+    std::vector<char*> av;
+    for (auto& s : a) av.push_back(const_cast<char*>(s.c_str()));
+    av.push_back(nullptr);
+    Grid par = parseArgs((int)a.size(), av.data());
+
+    int gsize = n * n * (dim == 3 ? n : 1);
+    double2* wfc = (double2*)malloc(sizeof(double2) * gsize);
+    {
+        FILE* f = fopen(get("psi0", "psi0.bin").c_str(), "rb");
+        if (!f || fread(wfc, sizeof(double2), gsize, f) != (size_t)gsize) {
+            fprintf(stderr, "cannot read psi0\n");
+            return 2;
+        }
+        fclose(f);
+        double s = std::pow(L, -0.5 * dim);
+        for (int i = 0; i < gsize; ++i) { wfc[i].x *= s; wfc[i].y *= s; }
+    }
+    par.store("read_wfc", true);
+    par.store("wfc", wfc);
+    int every = geti("energy_every", 0);
+    par.store("energy_calc", true);
+    par.store("energy_calc_steps", every > 0 ? every : 1 << 30);
+    par.store("energy_calc_threshold", getd("threshold", -1.0));
+    par.store("energy", 0.0);
+
+    init(par);
+    double gN = getd("g", 0) * HBAR * std::pow(L, dim);
+    par.store("interaction", gN / par.dval("gDenConst"));
+
+    std::string buf;
+    std::string out = get("out", "ref");
+    if (gsteps > 0) {
+        set_variables(par, 0);
+        cudaDeviceSynchronize();
+        auto t0 = std::chrono::steady_clock::now();
+        evolve(par, gsteps, 0, buf);
+        cudaDeviceSynchronize();
+        double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        dump(par, out + "_imag", gsize, L, dim, s);
+    }
+    if (esteps > 0) {
+        set_variables(par, 1);
+        cudaDeviceSynchronize();
+        auto t0 = std::chrono::steady_clock::now();
+        evolve(par, esteps, 1, buf);
+        cudaDeviceSynchronize();
+        double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        dump(par, out + "_real", gsize, L, dim, s);
+    }
+    return 0;
+}

@@ -1,0 +1,102 @@
+"""Seeded parity cases shared by the golden-fixture generator and the tests.
+
+Every case is a GPUE run in hbar = m = 1 units on a square/cubic grid
+x_i = -box + i*dx, dx = box/(n/2) (GPUE's generate_p_space), with a harmonic
+trap, optional rotation gauge A = omega*(-y wx, x wy) and optional nonlinear
+term.  Initial wavefunctions are built from numpy PCG64 streams so the
+fixtures only need to store outputs; each fixture records a checksum of its
+input so a change in the generator is caught.
+"""
+
+import hashlib
+
+import numpy as np
+
+CASES = {
+    # 2D imaginary time, nonlinear, renormalised every step
+    "g2d_imag_n64": dict(dim=2, n=64, box=10.0, g=100.0, gsteps=500, seed=11,
+                         init="gauss", energy_every=100),
+    # 2D imaginary time with the rotation gauge (imaginary-time gauge operators)
+    "g2d_imag_gauge_n64": dict(dim=2, n=64, box=8.0, g=200.0, omega=0.5, gauge=True,
+                               gsteps=400, seed=12, init="gauss", energy_every=100),
+    # 2D real time with the rotation gauge, both gauge orders alternate
+    "g2d_real_gauge_n64": dict(dim=2, n=64, box=8.0, g=200.0, omega=0.7, gauge=True,
+                               dt=5e-5, esteps=400, seed=13, init="phase", energy_every=100),
+    # 2D real time, linear Schroedinger, anisotropic trap
+    "g2d_real_lin_n32": dict(dim=2, n=32, box=6.0, wy=1.3, gpe=False, dt=1e-4, esteps=300,
+                             seed=14, init="phase", energy_every=100),
+    # 3D imaginary time, anisotropic trap
+    "g3d_imag_n16": dict(dim=3, n=16, box=6.0, wz=4.0, g=100.0, gsteps=200, seed=15,
+                         init="gauss", energy_every=50),
+    # 3D real time with the gauge (x,y,z then z,y,x orders)
+    "g3d_real_gauge_n16": dict(dim=3, n=16, box=6.0, wz=2.0, g=50.0, omega=0.5, gauge=True,
+                               dt=1e-4, esteps=200, seed=16, init="phase", energy_every=50),
+    # 3D imaginary time with the gauge
+    "g3d_imag_gauge_n32": dict(dim=3, n=32, box=6.0, wz=2.0, g=100.0, omega=0.3, gauge=True,
+                               gsteps=100, seed=17, init="gauss", energy_every=50),
+    # 256^2, g=100, gdt=1e-4, 10000 imaginary steps
+    "cfg1_256_imag": dict(dim=2, n=256, box=10.0, g=100.0, gsteps=10000, seed=1,
+                          init="gauss", energy_every=1000),
+}
+
+# Full-size configurations timed on GPUE's own build (make_golden.py --timing):
+# configs[0..2] shapes with the step counts used for timing.
+CASES.update({
+    "cfg2_1024_real_gauge": dict(dim=2, n=1024, box=16.0, g=500.0, omega=0.7, gauge=True,
+                                 dt=5e-5, esteps=20000, seed=2, init="phase"),
+    "cfg3_256_imag": dict(dim=3, n=256, box=12.0, wz=4.0, g=1000.0, gsteps=5000, seed=3,
+                          init="gauss"),
+})
+TIMING = [("cfg1_256_imag", 10000), ("cfg2_1024_real_gauge", 1000), ("cfg3_256_imag", 100)]
+FIXTURES = [k for k in CASES if not k.startswith(("cfg2", "cfg3"))]
+
+DEFAULTS = dict(wx=1.0, wy=1.0, wz=1.0, gamma=1.0, g=0.0, gpe=True, omega=0.0, gauge=False,
+                gdt=1e-4, dt=1e-4, gsteps=0, esteps=0, energy_every=0)
+
+
+def case(name):
+    c = dict(DEFAULTS)
+    c.update(CASES[name])
+    return c
+
+
+def coords(c):
+    n, box = c["n"], c["box"]
+    dx = box / (n >> 1)
+    x = -box + dx * np.arange(n)
+    return x, dx
+
+
+def initial_psi(c):
+    """complex128 array shaped (n, n) or (n, n, n) [z, y, x], normalised."""
+    dim, n = c["dim"], c["n"]
+    x, dx = coords(c)
+    rng = np.random.Generator(np.random.PCG64(c["seed"]))
+    grids = np.meshgrid(*([x] * dim), indexing="ij")
+    r2 = sum(gi * gi for gi in grids)
+    psi = np.exp(-r2 / 2.0) * (1.0 + 0.01 * rng.standard_normal(r2.shape))
+    psi = psi.astype(np.complex128)
+    if c["init"] == "phase":
+        theta = 2 * np.pi * rng.random(r2.shape)
+        k = 2 * np.pi * np.fft.fftfreq(n, d=dx)
+        kg = np.meshgrid(*([k] * dim), indexing="ij")
+        k2 = sum(ki * ki for ki in kg)
+        sm = np.real(np.fft.ifftn(np.fft.fftn(theta) * np.exp(-0.5 * k2 * 0.25)))
+        psi = psi * np.exp(1j * sm)
+    dV = dx ** dim
+    psi /= np.sqrt(np.sum(np.abs(psi) ** 2) * dV)
+    return np.ascontiguousarray(psi)
+
+
+def checksum(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()[:16]
+
+
+def harness_args(c, psi0_path, out_prefix, data_dir):
+    a = ["dim=%d" % c["dim"], "n=%d" % c["n"], "box=%r" % c["box"], "wx=%r" % c["wx"],
+         "wy=%r" % c["wy"], "wz=%r" % c["wz"], "gamma=%r" % c["gamma"], "g=%r" % c["g"],
+         "gpe=%d" % int(c["gpe"]), "omega=%r" % c["omega"], "gauge=%d" % int(c["gauge"]),
+         "gdt=%r" % c["gdt"], "dt=%r" % c["dt"], "gsteps=%d" % c["gsteps"],
+         "esteps=%d" % c["esteps"], "energy_every=%d" % c["energy_every"],
+         "psi0=" + psi0_path, "out=" + out_prefix, "data=" + data_dir]
+    return a

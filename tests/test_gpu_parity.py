@@ -1,0 +1,119 @@
+"""The CUDA path (through the C ABI) against GPUE's own build and the oracle.
+
+Plain FP64 form: wavefunction L2 <= 1e-12 and relative energy <= 1e-12
+against the golden fixtures made by GPUE's CUDA build.  Fused FP32 form:
+relative energy <= 1e-6 for imaginary-time (ground-state) runs and <= 2e-6
+for real-time runs, wavefunction L2 <= 2e-5 (complex64 rounding, FP64
+reductions).
+"""
+import numpy as np
+import pytest
+
+import cases
+from helpers import l2, load_golden, oracle_problem, run_product, steps_gstate
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def G():
+    import gpue_b200
+    return gpue_b200
+
+
+@pytest.mark.parametrize("name", cases.FIXTURES)
+def test_fp64_matches_reference_build(G, name):
+    ref, meta = load_golden(name)
+    c = cases.case(name)
+    psi, E, r = run_product(c, G.PREC_FP64)
+    steps, gs = steps_gstate(c)
+    assert r["steps_done"] == steps
+    assert l2(psi, ref, c) <= 1e-12
+    assert abs(E - meta["energy"]) <= 1e-12 * abs(meta["energy"])
+    assert abs(r["energy"] - meta["last_check_energy"]) <= 1e-12 * abs(meta["last_check_energy"])
+    assert r["kernel_launches"] > 0
+
+
+@pytest.mark.parametrize("name", cases.FIXTURES)
+def test_fp32_fused_close_to_reference_build(G, name):
+    ref, meta = load_golden(name)
+    c = cases.case(name)
+    psi, E, r = run_product(c, G.PREC_FP32)
+    steps, gs = steps_gstate(c)
+    tol_e = 1e-6 if gs == 0 else 2e-6
+    assert abs(E - meta["energy"]) <= tol_e * abs(meta["energy"])
+    assert l2(psi, ref, c) <= 2e-5
+
+
+MIXED = [
+    # non-power-of-two lengths (radix 3 and 5) that GPUE's reduction cannot run
+    dict(dim=2, n=96, box=8.0, g=80.0, gsteps=150, seed=21, init="gauss", energy_every=50),
+    dict(dim=2, n=192, box=8.0, g=150.0, omega=0.6, gauge=True, dt=5e-5, esteps=120, seed=22,
+         init="phase", energy_every=40),
+    dict(dim=2, n=160, box=8.0, g=50.0, omega=0.4, gauge=True, gsteps=100, seed=23,
+         init="gauss", energy_every=50),
+    dict(dim=2, n=384, box=12.0, g=300.0, wy=1.2, dt=5e-5, esteps=60, seed=24, init="phase",
+         energy_every=30),
+    dict(dim=3, n=32, box=6.0, wz=3.0, g=40.0, omega=0.5, gauge=True, dt=1e-4, esteps=60,
+         seed=25, init="phase", energy_every=30),
+    dict(dim=3, n=96, box=6.0, wz=2.0, g=60.0, gsteps=20, seed=26, init="gauss",
+         energy_every=10),
+]
+
+
+@pytest.mark.parametrize("k", range(len(MIXED)))
+def test_fp64_matches_oracle_mixed_sizes(G, k):
+    c = dict(cases.DEFAULTS)
+    c.update(MIXED[k])
+    psi0 = cases.initial_psi(c)
+    steps, gs = steps_gstate(c)
+    P = oracle_problem(c)
+    ref, res, en = P.evolve(psi0, steps, gs)
+    psi, E, r = run_product(c, G.PREC_FP64, psi0=psi0)
+    assert l2(psi, ref, c) <= 1e-12
+    Eref = P.energy(ref)
+    assert abs(E - Eref) <= 1e-12 * abs(Eref)
+    assert r["n_energies"] == res["n_energies"]
+    assert abs(r["energy"] - en[-1]) <= 1e-12 * abs(en[-1])
+    psi32, E32, _ = run_product(c, G.PREC_FP32, psi0=psi0)
+    assert abs(E32 - Eref) <= 2e-6 * abs(Eref)
+
+
+def test_energy_and_norm_of_initial_state(G):
+    c = cases.case("g2d_real_gauge_n64")
+    psi0 = cases.initial_psi(c)
+    P = oracle_problem(c)
+    from helpers import product_params
+    with G.Solver(product_params(c, G.PREC_FP64)) as s:
+        s.set_wfc(psi0)
+        s.set_operators(1)
+        assert abs(s.energy() - P.energy(psi0)) <= 1e-13 * abs(P.energy(psi0))
+        assert abs(s.norm() - 1.0) <= 1e-14
+        back = s.get_wfc()
+        assert np.array_equal(back, psi0)
+
+
+def test_early_stop_follows_gpue_rule(G):
+    """|E_old - E| < thr * E_old at check steps stops imaginary time
+    (src/evolution.cu:891-902) at the same step as the oracle."""
+    c = dict(cases.DEFAULTS, dim=2, n=64, box=6.0, g=20.0, gsteps=4000, seed=31, init="gauss",
+             energy_every=100, gdt=1e-3)
+    psi0 = cases.initial_psi(c)
+    P = oracle_problem(c, threshold=1e-7)
+    ref, res, en = P.evolve(psi0, 4000, 0)
+    assert res["early_stop"] == 1
+    psi, E, r = run_product(c, G.PREC_FP64, psi0=psi0, threshold=1e-7)
+    assert r["early_stop"] == 1 and r["steps_done"] == res["steps_done"]
+    assert l2(psi, ref, c) <= 1e-12
+
+
+def test_fp32_roundtrip_and_dtypes(G):
+    c = cases.case("g2d_imag_n64")
+    psi0 = cases.initial_psi(c)
+    from helpers import product_params
+    with G.Solver(product_params(c, G.PREC_FP32)) as s:
+        s.set_wfc(psi0)
+        b64 = s.get_wfc(np.complex64)
+        assert np.array_equal(b64, psi0.astype(np.complex64))
+        b128 = s.get_wfc(np.complex128)
+        assert np.array_equal(b128, psi0.astype(np.complex64).astype(np.complex128))
