@@ -53,6 +53,9 @@ def parse_args():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="skip the steady-state and e2e legs")
+    ap.add_argument("--profile", choices=["fp32", "fp64"], default=None,
+                    help="profiling case for ncu: the same workload without the relaxation "
+                         "prep, --warmup + --steps time steps of one form, no timing output")
     return ap.parse_args()
 
 
@@ -299,10 +302,32 @@ def reference_arm(args):
 
 # ------------------------------------------------------------- main -------
 
+def profile_case(args):
+    """Small deterministic run for ncu captures (same kernels as the timed leg)."""
+    import numpy as np
+    import gpue_b200 as G
+    n, box = WORK["n"], WORK["box"]
+    dx = box / (n >> 1)
+    x = -box + dx * np.arange(n)
+    psi0 = (np.exp(-(x[None, :] ** 2 + x[:, None] ** 2) / 8.0) *
+            np.exp(1j * phase_field(n, box))).astype(np.complex128)
+    prec = G.PREC_FP32 if args.profile == "fp32" else G.PREC_FP64
+    with G.Solver(work_params(G, prec, 0)) as s:
+        s.set_wfc(psi0)
+        r0 = s.evolve(args.warmup * STEPS_PER_BENCH_STEP, 1)
+        r1 = s.evolve(args.steps * STEPS_PER_BENCH_STEP, 1,
+                      step_offset=args.warmup * STEPS_PER_BENCH_STEP)
+    print(json.dumps({"profile": args.profile, "warmup_launches": r0["kernel_launches"],
+                      "launches": r1["kernel_launches"], "device_ms": r1["device_ms"]}))
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         reference_arm(args)
+        return
+    if args.profile:
+        profile_case(args)
         return
     import torch
     import gpue_b200 as G

@@ -14,7 +14,12 @@
 //   2D gauge 0  R[scale? V/2 F]  C[F K I]  R[I V/2]  C[F Gy I]  R[F Gx I] (+norm)
 //   3D          X[scale? V/2 F]  Y[F]  Z[F K I]  Y[I]  X[I V/2] (+gauge passes)
 // In real time the last pass of a step and the first pass of the next are
-// fused when they share an axis (no renormalisation lies between them).
+// fused when they share an axis (no renormalisation lies between them).  The
+// z gauge pass is left out: Az = 0 for the rotation gauge.
+//
+// An FP32-form context keeps an FP64 shadow of the state for the polishing
+// steps that end an imaginary-time run; after a polish the FP64 state is the
+// authoritative one until the next FP32 evolve.
 
 #include <cuda_runtime.h>
 
@@ -46,8 +51,8 @@ struct Axis {
 // Device tables for one precision.
 struct Tables {
     void* buf = nullptr;
-    const void* vfac[3] = {};
-    const void* kfac[3] = {};
+    const double2* vfac[3] = {};
+    const double2* kfac[3] = {};
     const void* tw[3] = {};
     const double* pos[3] = {};
     const double* mom[3] = {};
@@ -55,8 +60,15 @@ struct Tables {
     int built_for = -1;  // gstate of vfac/kfac
 };
 
+struct LaunchCfg {
+    const PassKernel* k = nullptr;
+    int threads = 0, blocks = 0;
+    long ntiles = 0;
+    size_t smem = 0;
+};
+
 struct GraphKey {
-    int gstate, parity, nsteps, scale_first, energy_last;
+    int prec, gstate, parity, nsteps, scale_first, energy_last, guard;
     bool operator<(const GraphKey& o) const {
         return std::memcmp(this, &o, sizeof(GraphKey)) < 0;
     }
@@ -77,29 +89,44 @@ struct gpue_ctx {
     long N = 0;
     double dV = 1;
     int device = 0;
+    int sms = 148;
     cudaStream_t stream = nullptr;
     void* psi = nullptr;      // resident state in the context precision
+    void* psi64 = nullptr;    // FP64 shadow of an FP32 context (polishing)
+    bool polished = false;    // psi64 holds the authoritative state
     void* scratch = nullptr;  // N * 16 bytes
     double* scal = nullptr;   // device scalars
     double2* partials = nullptr;
     long partials_cap = 0;
     unsigned* counters = nullptr;
-    Tables tab[2];  // [PREC_F64], [PREC_F32]
+    Tables tab[2];            // indexed by GPUE_PREC_*
+    LaunchCfg lc[2][3];       // [precision][axis]
     bool have_wfc = false;
     bool pending_scale = false;  // scal[kScale] must multiply psi
     std::map<GraphKey, Segment> graphs;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::string err;
-    long launches = 0;  // kernels enqueued in the current evolve call
+    long launches = 0;         // kernels enqueued in the current evolve call
     double last_energy = 0.0;  // energy of the latest check (GPUE's "energy" key)
 };
 
 namespace {
 
 // device scalar slots
-enum { kScale = 0, kEkin = 1, kEreal = 2, kNorm = 3, kNScal = 8 };
-// counter slots (one per reduction that may be in flight in a graph)
+enum {
+    kScale = 0,       // imaginary-time renormalisation factor
+    kEkin = 1,
+    kEreal = 2,
+    kNorm = 3,
+    kGuard = 4,       // real-time norm-guard factor
+    kTargetImag = 5,  // 1/dV: sum |psi|^2 of a unit-norm state
+    kTargetReal = 6,  // sum |psi|^2 at the start of a real-time evolve
+    kOne = 7,
+    kNScal = 8
+};
+// counter slots: reductions in flight in one stream use distinct counters
 enum { kCtrNorm = 0, kCtrEkin = 1, kCtrEreal = 2, kCtrMisc = 3, kNCtr = 8 };
+constexpr long kAuxPartials = 4096;  // partials reserved for the aux kernels
 
 gpue_status fail(gpue_ctx* c, gpue_status st, const char* fmt, ...) {
     if (c) {
@@ -124,6 +151,11 @@ gpue_status fail(gpue_ctx* c, gpue_status st, const char* fmt, ...) {
     } while (0)
 
 size_t elem_size(int prec) { return prec == GPUE_PREC_FP32 ? 8 : 16; }
+int kprec(int prec) { return prec == GPUE_PREC_FP32 ? PREC_F32 : PREC_F64; }
+
+void* state_of(gpue_ctx* c, int prec) {
+    return prec == c->prec ? c->psi : c->psi64;
+}
 
 // generate_p_space for one axis (src/operators.cu:336-343; init.cu:140-161)
 void build_axis(Axis& a, int n, double xmax, bool active) {
@@ -188,31 +220,24 @@ void axis_potential(const gpue_ctx* c, int a, std::vector<double>& v) {
     }
 }
 
-template <typename T>
-struct HostCx {
-    T x, y;
-};
-
 // Build tables for precision `prec` and time type gstate (aux_fields,
-// src/operators.cu:1069-1111, per axis).
+// src/operators.cu:1069-1111, per axis).  Factors are FP64 in both forms;
+// the DFT twiddles are in the storage precision.
 gpue_status build_tables(gpue_ctx* c, int prec, int gstate) {
     Tables& tb = c->tab[prec];
     if (tb.built_for == gstate) return GPUE_OK;
     const gpue_params& p = c->p;
     const size_t es = elem_size(prec);
-    // layout: per axis [vfac n][kfac n][tw n] complex, then [pos n][mom n][vreal n] double
+    auto al = [](size_t b) { return ((b + 255) / 256) * 256; };
+    // per axis: [vfac][kfac] double2, [tw] storage complex, [pos][mom][vreal] double
     size_t off = 0;
     size_t offs[3][6];
     for (int a = 0; a < 3; ++a) {
-        const int n = c->ax[a].n;
-        for (int k = 0; k < 3; ++k) {
-            offs[a][k] = off;
-            off += ((n * es + 255) / 256) * 256;
-        }
-        for (int k = 3; k < 6; ++k) {
-            offs[a][k] = off;
-            off += ((n * 8 + 255) / 256) * 256;
-        }
+        const size_t n = c->ax[a].n;
+        offs[a][0] = off; off += al(n * 16);
+        offs[a][1] = off; off += al(n * 16);
+        offs[a][2] = off; off += al(n * es);
+        for (int k = 3; k < 6; ++k) { offs[a][k] = off; off += al(n * 8); }
     }
     if (!tb.buf) CK(cudaMalloc(&tb.buf, off));
     std::vector<unsigned char> h(off, 0);
@@ -221,30 +246,31 @@ gpue_status build_tables(gpue_ctx* c, int prec, int gstate) {
         const int n = A.n;
         std::vector<double> va;
         axis_potential(c, a, va);
+        double* vf = (double*)(h.data() + offs[a][0]);
+        double* kf = (double*)(h.data() + offs[a][1]);
         for (int i = 0; i < n; ++i) {
             const double K = (p.hbar * p.hbar / (2 * p.mass)) * (A.p[i] * A.p[i]);
-            double vr, vi, kr, ki;
             if (gstate == 0) {
-                vr = std::exp(-va[i] * (p.gdt / (2 * p.hbar)));
-                vi = 0.0;
-                kr = std::exp(-K * (p.gdt / p.hbar));
-                ki = 0.0;
+                vf[2 * i] = std::exp(-va[i] * (p.gdt / (2 * p.hbar)));
+                vf[2 * i + 1] = 0.0;
+                kf[2 * i] = std::exp(-K * (p.gdt / p.hbar));
+                kf[2 * i + 1] = 0.0;
             } else {
-                vr = std::cos(-va[i] * (p.dt / (2 * p.hbar)));
-                vi = std::sin(-va[i] * (p.dt / (2 * p.hbar)));
-                kr = std::cos(-K * (p.dt / p.hbar));
-                ki = std::sin(-K * (p.dt / p.hbar));
+                vf[2 * i] = std::cos(-va[i] * (p.dt / (2 * p.hbar)));
+                vf[2 * i + 1] = std::sin(-va[i] * (p.dt / (2 * p.hbar)));
+                kf[2 * i] = std::cos(-K * (p.dt / p.hbar));
+                kf[2 * i + 1] = std::sin(-K * (p.dt / p.hbar));
             }
             const long double ang = -2.0L * 3.141592653589793238462643383279L * i / n;
             const double twr = (double)cosl(ang), twi = (double)sinl(ang);
             if (prec == GPUE_PREC_FP32) {
-                ((HostCx<float>*)(h.data() + offs[a][0]))[i] = {(float)vr, (float)vi};
-                ((HostCx<float>*)(h.data() + offs[a][1]))[i] = {(float)kr, (float)ki};
-                ((HostCx<float>*)(h.data() + offs[a][2]))[i] = {(float)twr, (float)twi};
+                float* tw = (float*)(h.data() + offs[a][2]);
+                tw[2 * i] = (float)twr;
+                tw[2 * i + 1] = (float)twi;
             } else {
-                ((HostCx<double>*)(h.data() + offs[a][0]))[i] = {vr, vi};
-                ((HostCx<double>*)(h.data() + offs[a][1]))[i] = {kr, ki};
-                ((HostCx<double>*)(h.data() + offs[a][2]))[i] = {twr, twi};
+                double* tw = (double*)(h.data() + offs[a][2]);
+                tw[2 * i] = twr;
+                tw[2 * i + 1] = twi;
             }
             ((double*)(h.data() + offs[a][3]))[i] = A.x[i];
             ((double*)(h.data() + offs[a][4]))[i] = A.p[i];
@@ -255,8 +281,8 @@ gpue_status build_tables(gpue_ctx* c, int prec, int gstate) {
     CK(cudaStreamSynchronize(c->stream));
     unsigned char* b = (unsigned char*)tb.buf;
     for (int a = 0; a < 3; ++a) {
-        tb.vfac[a] = b + offs[a][0];
-        tb.kfac[a] = b + offs[a][1];
+        tb.vfac[a] = (const double2*)(b + offs[a][0]);
+        tb.kfac[a] = (const double2*)(b + offs[a][1]);
         tb.tw[a] = b + offs[a][2];
         tb.pos[a] = (const double*)(b + offs[a][3]);
         tb.mom[a] = (const double*)(b + offs[a][4]);
@@ -268,29 +294,14 @@ gpue_status build_tables(gpue_ctx* c, int prec, int gstate) {
 
 // ---------------------------------------------------------------- passes --
 
-struct LPass {
-    int axis;
-    std::vector<int> ops;
-    int red;          // RED_NONE / RED_NORM / RED_SUM
-    int red_slot;     // scalar slot for the result
-    int ctr;          // counter slot
-    bool store = true;
-    bool to_scratch = false;   // out = scratch
-    bool from_scratch = false; // in = scratch
-    double gauge_dt = 0;       // for OP_GAUGE
-};
-
-struct LaunchCfg {
-    const PassKernel* k;
-    int threads, blocks;
-    size_t smem;
-};
-
-gpue_status pass_launch_cfg(gpue_ctx* c, int prec, int axis, LaunchCfg& lc) {
+// Launch shape for one precision and axis: C lines per tile, a persistent
+// grid of (resident CTAs per SM) x SMs walking the tiles.
+gpue_status plan_axis(gpue_ctx* c, int prec, int axis) {
+    LaunchCfg& lc = c->lc[prec][axis];
     const int n = c->ax[axis].n;
-    const PassKernel* k = find_pass_kernel(prec, n);
+    const PassKernel* k = find_pass_kernel(kprec(prec), n);
     if (!k) return fail(c, GPUE_ERR_UNSUPPORTED, "no FFT plan for length %d", n);
-    long nlines = c->N / n;
+    const long nlines = c->N / n;
     int C;
     if (axis == 0) {
         C = 128 / k->p;
@@ -305,38 +316,55 @@ gpue_status pass_launch_cfg(gpue_ctx* c, int prec, int axis, LaunchCfg& lc) {
     while (C > 1 && nlines % C) C >>= 1;
     lc.k = k;
     lc.threads = C * k->p;
-    lc.blocks = (int)(nlines / C);
-    const size_t tsz = k->elem / 2;
-    lc.smem = (size_t)C * 2 * k->ls * tsz;
+    lc.ntiles = nlines / C;
+    lc.smem = (size_t)C * k->ls * k->elem;
     const size_t red_need = 2 * ((lc.threads + 31) / 32) * sizeof(double);
     if (lc.smem < red_need) lc.smem = red_need;
-    return GPUE_OK;
-}
-
-gpue_status set_smem_attr(gpue_ctx* c, const LaunchCfg& lc, int axis) {
-    void* fn = axis == 0 ? (void*)lc.k->row : (void*)lc.k->col;
+    void* fn = axis == 0 ? (void*)k->row : (void*)k->col;
     if (lc.smem > 48 * 1024)
         CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lc.smem));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, lc.threads, lc.smem));
+    if (per_sm < 1) per_sm = 1;
+    long blocks = (long)per_sm * c->sms;
+    if (blocks > lc.ntiles) blocks = lc.ntiles;
+    lc.blocks = (int)blocks;
     return GPUE_OK;
 }
 
+struct LPass {
+    int axis = 0;
+    std::vector<int> ops;
+    int red = RED_NONE;       // RED_NONE / RED_NORM / RED_SUM
+    bool red_blocks = true;   // the next pass needs the reduction result
+    int red_slot = 0;         // scalar slot for the result
+    int red_target = kTargetImag;
+    int ctr = 0;              // counter slot
+    bool store = true;
+    bool to_scratch = false;   // out = scratch
+    bool from_scratch = false; // in = scratch
+    double gauge_dt = 0;       // for OP_GAUGE
+    int scale_slot = kScale;   // OP_SCALE factor
+    int kscale_slot = -1;      // extra factor folded into OP_KPHASE (norm guard)
+};
+
 gpue_status launch_pass(gpue_ctx* c, int prec, const LPass& lp, int gstate) {
-    LaunchCfg lc;
-    gpue_status st = pass_launch_cfg(c, prec, lp.axis, lc);
-    if (st) return st;
-    if (lp.red != RED_NONE && lc.blocks > c->partials_cap)
+    const LaunchCfg& lc = c->lc[prec][lp.axis];
+    if (!lc.k) return fail(c, GPUE_ERR_STATE, "axis %d not planned", lp.axis);
+    if (lp.red != RED_NONE && lc.blocks > c->partials_cap - kAuxPartials)
         return fail(c, GPUE_ERR_INVALID_ARG, "reduction grid %d exceeds scratch", lc.blocks);
     const Tables& tb = c->tab[prec];
     const gpue_params& p = c->p;
     PassArgs a;
     std::memset(&a, 0, sizeof a);
-    void* psi = (prec == c->prec) ? c->psi : nullptr;
+    void* psi = state_of(c, prec);
     a.in = lp.from_scratch ? c->scratch : psi;
-    a.out = lp.to_scratch ? c->scratch : (lp.from_scratch ? c->scratch : psi);
+    a.out = (lp.to_scratch || lp.from_scratch) ? c->scratch : psi;
     a.axis = lp.axis;
     a.nx = c->ax[0].n;
     a.ny = c->ax[1].n;
     a.nz = c->ax[2].n;
+    a.ntiles = lc.ntiles;
     a.nops = (int)lp.ops.size();
     for (int i = 0; i < a.nops; ++i) a.ops[i] = lp.ops[i];
     a.store = lp.store ? 1 : 0;
@@ -344,19 +372,14 @@ gpue_status launch_pass(gpue_ctx* c, int prec, const LPass& lp, int gstate) {
     a.gpe = p.gpe;
     const double Dt = gstate == 0 ? p.gdt : p.dt;
     a.nl_coef = (p.interaction * p.gDenConst) * ((0.5 * Dt) / p.hbar);
+    a.kscale = 1.0 / (double)c->N;
+    a.gscale = 1.0 / (double)c->ax[lp.axis].n;
     double axc, ayc;
     gauge_coefs(c, axc, ayc);
-    if (lp.axis == 0) {
-        a.gauge_coef = axc;
-        a.gauge_src = 1;
-    } else if (lp.axis == 1) {
-        a.gauge_coef = ayc;
-        a.gauge_src = 0;
-    } else {
-        a.gauge_coef = 0.0;
-        a.gauge_src = 0;
-    }
+    a.gauge_coef = lp.axis == 0 ? axc : lp.axis == 1 ? ayc : 0.0;
+    a.gauge_src = lp.axis == 0 ? 1 : 0;
     a.gauge_dt = lp.gauge_dt;
+    a.dmom = c->ax[lp.axis].n > 1 ? c->ax[lp.axis].p[1] : 0.0;
     a.kin_coef = p.hbar * p.hbar / (2 * p.mass);
     for (int i = 0; i < 3; ++i) {
         a.vfac[i] = tb.vfac[i];
@@ -365,13 +388,13 @@ gpue_status launch_pass(gpue_ctx* c, int prec, const LPass& lp, int gstate) {
         a.mom[i] = tb.mom[i];
     }
     a.tw = tb.tw[lp.axis];
-    a.inv_sqrt_n = 1.0 / std::pow((double)c->ax[lp.axis].n, 0.5);
     a.red.kind = lp.red;
     a.red.partials = c->partials;
     a.red.counter = c->counters + lp.ctr;
     a.red.out = c->scal + lp.red_slot;
-    a.red.dV = c->dV;
-    a.scale_in = c->scal + kScale;
+    a.red.target = c->scal + lp.red_target;
+    a.scale_in = c->scal + lp.scale_slot;
+    a.kscale_in = lp.kscale_slot >= 0 ? c->scal + lp.kscale_slot : nullptr;
     void (*fn)(PassArgs) = lp.axis == 0 ? lc.k->row : lc.k->col;
     fn<<<lc.blocks, lc.threads, lc.smem, c->stream>>>(a);
     c->launches++;
@@ -379,8 +402,9 @@ gpue_status launch_pass(gpue_ctx* c, int prec, const LPass& lp, int gstate) {
     return GPUE_OK;
 }
 
-// Logical passes of step i (see the file header).
-void step_passes(gpue_ctx* c, int i, int gstate, bool scale_first, double rexp,
+// Logical passes of step i (see the file header).  guard: real-time norm
+// guard (NORM on the last pass, factor folded into the next K).
+void step_passes(gpue_ctx* c, int i, int gstate, bool scale_first, double rexp, bool guard,
                  std::vector<LPass>& out) {
     const bool imag = gstate == 0;
     const bool g = gauge_active(c);
@@ -389,9 +413,6 @@ void step_passes(gpue_ctx* c, int i, int gstate, bool scale_first, double rexp,
         LPass lp;
         lp.axis = axis;
         lp.ops = ops;
-        lp.red = RED_NONE;
-        lp.red_slot = 0;
-        lp.ctr = 0;
         lp.gauge_dt = gdt;
         return lp;
     };
@@ -401,41 +422,30 @@ void step_passes(gpue_ctx* c, int i, int gstate, bool scale_first, double rexp,
     first.push_back(OP_VHALF);
     first.push_back(OP_FFT_F);
     const bool flip = (i % 2) != 0;
-    if (c->dim == 2) {
-        s.push_back(P(0, first));
-        s.push_back(P(1, {OP_FFT_F, OP_KPHASE, OP_FFT_I}));
-        if (g && flip) {
-            s.push_back(P(0, {OP_FFT_I, OP_VHALF, OP_FFT_F, OP_GAUGE, OP_FFT_I}));
-            s.push_back(P(1, {OP_FFT_F, OP_GAUGE, OP_FFT_I}));
-        } else if (g) {
-            s.push_back(P(0, {OP_FFT_I, OP_VHALF}));
-            s.push_back(P(1, {OP_FFT_F, OP_GAUGE, OP_FFT_I}));
-            s.push_back(P(0, {OP_FFT_F, OP_GAUGE, OP_FFT_I}));
-        } else {
-            s.push_back(P(0, {OP_FFT_I, OP_VHALF}));
-        }
+    const int kaxis = c->dim == 3 ? 2 : 1;
+    s.push_back(P(0, first));
+    if (c->dim == 3) s.push_back(P(1, {OP_FFT_F}));
+    LPass kp = P(kaxis, {OP_FFT_F, OP_KPHASE, OP_FFT_I});
+    if (guard) kp.kscale_slot = kGuard;
+    s.push_back(kp);
+    if (c->dim == 3) s.push_back(P(1, {OP_FFT_I}));
+    if (g && flip) {
+        s.push_back(P(0, {OP_FFT_I, OP_VHALF, OP_FFT_F, OP_GAUGE, OP_FFT_I}));
+        s.push_back(P(1, {OP_FFT_F, OP_GAUGE, OP_FFT_I}));
+    } else if (g) {
+        s.push_back(P(0, {OP_FFT_I, OP_VHALF}));
+        s.push_back(P(1, {OP_FFT_F, OP_GAUGE, OP_FFT_I}));
+        s.push_back(P(0, {OP_FFT_F, OP_GAUGE, OP_FFT_I}));
     } else {
-        s.push_back(P(0, first));
-        s.push_back(P(1, {OP_FFT_F}));
-        s.push_back(P(2, {OP_FFT_F, OP_KPHASE, OP_FFT_I}));
-        s.push_back(P(1, {OP_FFT_I}));
-        // Az = 0 for the rotation gauge: the z gauge pass is the identity
-        if (g && flip) {
-            s.push_back(P(0, {OP_FFT_I, OP_VHALF, OP_FFT_F, OP_GAUGE, OP_FFT_I}));
-            s.push_back(P(1, {OP_FFT_F, OP_GAUGE, OP_FFT_I}));
-        } else if (g) {
-            s.push_back(P(0, {OP_FFT_I, OP_VHALF}));
-            s.push_back(P(1, {OP_FFT_F, OP_GAUGE, OP_FFT_I}));
-            s.push_back(P(0, {OP_FFT_F, OP_GAUGE, OP_FFT_I}));
-        } else {
-            s.push_back(P(0, {OP_FFT_I, OP_VHALF}));
-        }
+        s.push_back(P(0, {OP_FFT_I, OP_VHALF}));
     }
-    if (imag) {
+    if (imag || guard) {
         LPass& last = s.back();
         last.ops.push_back(OP_NORM);
         last.red = RED_NORM;
-        last.red_slot = kScale;
+        last.red_slot = imag ? kScale : kGuard;
+        last.red_target = imag ? kTargetImag : kTargetReal;
+        last.red_blocks = imag;  // the guard factor is only read by the next K pass
         last.ctr = kCtrNorm;
     }
     for (auto& x : s) out.push_back(x);
@@ -447,16 +457,23 @@ void fuse(std::vector<LPass>& v) {
     for (auto& p : v) {
         if (!o.empty()) {
             LPass& q = o.back();
-            bool has_scale = false, q_gauge = false, p_gauge = false;
+            bool has_scale = false, q_gauge = false, p_gauge = false, p_red = false;
             for (int op : p.ops) has_scale |= (op == OP_SCALE), p_gauge |= (op == OP_GAUGE);
             for (int op : q.ops) q_gauge |= (op == OP_GAUGE);
-            if (q.axis == p.axis && q.red == RED_NONE && !has_scale && q.store && p.store &&
+            p_red = p.red != RED_NONE;
+            const bool q_red_ok = q.red == RED_NONE || (!q.red_blocks && !p_red);
+            if (q.axis == p.axis && q_red_ok && !has_scale && q.store && p.store &&
                 !q.to_scratch && !p.from_scratch && !(q_gauge && p_gauge) &&
+                q.kscale_slot < 0 && p.kscale_slot < 0 &&
                 q.ops.size() + p.ops.size() <= (size_t)kMaxOps) {
                 for (int op : p.ops) q.ops.push_back(op);
-                q.red = p.red;
-                q.red_slot = p.red_slot;
-                q.ctr = p.ctr;
+                if (p_red) {
+                    q.red = p.red;
+                    q.red_slot = p.red_slot;
+                    q.red_target = p.red_target;
+                    q.red_blocks = p.red_blocks;
+                    q.ctr = p.ctr;
+                }
                 if (p_gauge) q.gauge_dt = p.gauge_dt;
                 continue;
             }
@@ -466,31 +483,26 @@ void fuse(std::vector<LPass>& v) {
     v.swap(o);
 }
 
-// Energy passes: kinetic sum K|psi_k|^2 via a forward transform into scratch,
-// and the real-space terms.  scale_pending applies the deferred renorm.
+// Energy: kinetic sum K|psi_k|^2 via an unnormalised forward transform into
+// scratch (divided by N on the host), and the real-space terms.
 gpue_status launch_energy(gpue_ctx* c, int prec, int gstate, bool scale_pending) {
     std::vector<LPass> v;
-    auto P = [&](int axis, std::vector<int> ops) {
-        LPass lp;
-        lp.axis = axis;
-        lp.ops = ops;
-        lp.red = RED_NONE;
-        lp.red_slot = 0;
-        lp.ctr = 0;
-        return lp;
-    };
-    std::vector<int> f;
-    if (scale_pending) f.push_back(OP_SCALE);
-    f.push_back(OP_FFT_F);
-    LPass x = P(0, f);
+    LPass x;
+    x.axis = 0;
+    if (scale_pending) x.ops.push_back(OP_SCALE);
+    x.ops.push_back(OP_FFT_F);
     x.to_scratch = true;
     v.push_back(x);
     if (c->dim == 3) {
-        LPass y = P(1, {OP_FFT_F});
+        LPass y;
+        y.axis = 1;
+        y.ops = {OP_FFT_F};
         y.from_scratch = true;
         v.push_back(y);
     }
-    LPass last = P(c->dim == 3 ? 2 : 1, {OP_FFT_F, OP_EKIN});
+    LPass last;
+    last.axis = c->dim == 3 ? 2 : 1;
+    last.ops = {OP_FFT_F, OP_EKIN};
     last.from_scratch = true;
     last.store = false;
     last.red = RED_SUM;
@@ -504,7 +516,7 @@ gpue_status launch_energy(gpue_ctx* c, int prec, int gstate, bool scale_pending)
     const Tables& tb = c->tab[prec];
     EnergyArgs e;
     std::memset(&e, 0, sizeof e);
-    e.psi = c->psi;
+    e.psi = state_of(c, prec);
     e.N = c->N;
     e.nx = c->ax[0].n;
     e.ny = c->ax[1].n;
@@ -527,11 +539,10 @@ gpue_status launch_energy(gpue_ctx* c, int prec, int gstate, bool scale_pending)
     e.dz = c->ax[2].dx;
     e.hbar = c->p.hbar;
     e.red.kind = RED_SUM;
-    e.red.partials = c->partials + (c->partials_cap - 2048);
+    e.red.partials = c->partials + (c->partials_cap - kAuxPartials);
     e.red.counter = c->counters + kCtrEreal;
     e.red.out = c->scal + kEreal;
-    e.red.dV = c->dV;
-    const int blocks = 148 * 4;
+    const int blocks = c->sms * 4;
     if (prec == GPUE_PREC_FP32) k_energy_real<float><<<blocks, 256, 0, c->stream>>>(e);
     else k_energy_real<double><<<blocks, 256, 0, c->stream>>>(e);
     c->launches++;
@@ -543,50 +554,88 @@ gpue_status read_energy(gpue_ctx* c, double* E) {
     double h[kNScal];
     CK(cudaMemcpyAsync(h, c->scal, sizeof h, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    *E = (h[kEkin] + h[kEreal]) * c->dV;
+    *E = (h[kEkin] / (double)c->N + h[kEreal]) * c->dV;
     return GPUE_OK;
 }
 
-gpue_status apply_pending_scale(gpue_ctx* c) {
-    if (!c->pending_scale) return GPUE_OK;
-    if (c->prec == GPUE_PREC_FP32)
-        k_scale<float><<<148 * 8, 256, 0, c->stream>>>(c->psi, c->N, c->scal + kScale);
+gpue_status scale_state(gpue_ctx* c, int prec, int slot) {
+    void* psi = state_of(c, prec);
+    if (prec == GPUE_PREC_FP32)
+        k_scale<float><<<c->sms * 8, 256, 0, c->stream>>>(psi, c->N, c->scal + slot);
     else
-        k_scale<double><<<148 * 8, 256, 0, c->stream>>>(c->psi, c->N, c->scal + kScale);
+        k_scale<double><<<c->sms * 8, 256, 0, c->stream>>>(psi, c->N, c->scal + slot);
     c->launches++;
     CK(cudaGetLastError());
+    return GPUE_OK;
+}
+
+gpue_status apply_pending_scale(gpue_ctx* c, int prec) {
+    if (!c->pending_scale) return GPUE_OK;
+    gpue_status st = scale_state(c, prec, kScale);
+    if (st) return st;
     c->pending_scale = false;
     return GPUE_OK;
 }
 
+// sum |psi|^2 of a state into a scalar slot (stream-ordered, no sync)
+gpue_status norm_to_slot(gpue_ctx* c, int prec, int slot) {
+    RedArgs r;
+    std::memset(&r, 0, sizeof r);
+    r.kind = RED_SUM;
+    r.partials = c->partials + (c->partials_cap - kAuxPartials);
+    r.counter = c->counters + kCtrMisc;
+    r.out = c->scal + slot;
+    void* psi = state_of(c, prec);
+    if (prec == GPUE_PREC_FP32) k_norm<float><<<c->sms * 4, 256, 0, c->stream>>>(psi, c->N, r);
+    else k_norm<double><<<c->sms * 4, 256, 0, c->stream>>>(psi, c->N, r);
+    c->launches++;
+    CK(cudaGetLastError());
+    return GPUE_OK;
+}
+
+gpue_status norm_now(gpue_ctx* c, int prec, double* out) {
+    gpue_status st = norm_to_slot(c, prec, kNorm);
+    if (st) return st;
+    double h;
+    CK(cudaMemcpyAsync(&h, c->scal + kNorm, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    *out = h * c->dV;
+    return GPUE_OK;
+}
+
 // Enqueue steps [i0, i1) (+ energy passes after the last one when asked).
-gpue_status enqueue_steps(gpue_ctx* c, int i0, int i1, int gstate, bool scale_first,
-                          const std::vector<double>& rexp, bool energy_after) {
+gpue_status enqueue_steps(gpue_ctx* c, int prec, int i0, int i1, int gstate, bool scale_first,
+                          const std::vector<double>& rexp, bool energy_after, bool guard) {
     std::vector<LPass> v;
+    // every imaginary-time step after the first renormalises the state the
+    // previous step left (the deferred parSum scale)
     for (int i = i0; i < i1; ++i)
-        step_passes(c, i, gstate, scale_first && i == i0, rexp.empty() ? 1.0 : rexp[i], v);
-    if (gstate != 0) fuse(v);
+        step_passes(c, i, gstate, i == i0 ? scale_first : gstate == 0,
+                    rexp.empty() ? 1.0 : rexp[i], guard, v);
+    fuse(v);
     for (auto& lp : v) {
-        gpue_status st = launch_pass(c, c->prec, lp, gstate);
+        gpue_status st = launch_pass(c, prec, lp, gstate);
         if (st) return st;
     }
     if (energy_after) {
-        gpue_status st = launch_energy(c, c->prec, gstate, gstate == 0);
+        gpue_status st = launch_energy(c, prec, gstate, gstate == 0);
         if (st) return st;
     }
     return GPUE_OK;
 }
 
-gpue_status run_segment(gpue_ctx* c, int i0, int i1, int gstate, bool scale_first,
-                        const std::vector<double>& rexp, bool energy_after, bool use_graph) {
-    if (!use_graph || !rexp.empty())
-        return enqueue_steps(c, i0, i1, gstate, scale_first, rexp, energy_after);
-    GraphKey key{gstate, i0 % 2, i1 - i0, scale_first ? 1 : 0, energy_after ? 1 : 0};
+gpue_status run_segment(gpue_ctx* c, int prec, int i0, int i1, int gstate, bool scale_first,
+                        const std::vector<double>& rexp, bool energy_after, bool guard) {
+    if (!rexp.empty())
+        return enqueue_steps(c, prec, i0, i1, gstate, scale_first, rexp, energy_after, guard);
+    GraphKey key{prec, gstate, i0 % 2, i1 - i0, scale_first ? 1 : 0, energy_after ? 1 : 0,
+                 guard ? 1 : 0};
     auto it = c->graphs.find(key);
     if (it == c->graphs.end()) {
-        long before = c->launches;
+        const long before = c->launches;
         CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-        gpue_status st = enqueue_steps(c, i0, i1, gstate, scale_first, rexp, energy_after);
+        gpue_status st =
+            enqueue_steps(c, prec, i0, i1, gstate, scale_first, rexp, energy_after, guard);
         cudaGraph_t g = nullptr;
         cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
         if (st) {
@@ -613,20 +662,94 @@ void destroy_graphs(gpue_ctx* c) {
     c->graphs.clear();
 }
 
-gpue_status norm_now(gpue_ctx* c, double* out) {
-    RedArgs r;
-    r.kind = RED_SUM;
-    r.partials = c->partials + (c->partials_cap - 2048);
-    r.counter = c->counters + kCtrMisc;
-    r.out = c->scal + kNorm;
-    r.dV = c->dV;
-    if (c->prec == GPUE_PREC_FP32) k_norm<float><<<148 * 4, 256, 0, c->stream>>>(c->psi, c->N, r);
-    else k_norm<double><<<148 * 4, 256, 0, c->stream>>>(c->psi, c->N, r);
+struct LoopOut {
+    int done = 0, early = 0, n_en = 0;
+    double energy = NAN;
+};
+
+// The step loop of evolve() on the state of precision `prec`, absolute steps
+// [off, off + nsteps), energy checks and early stop as GPUE does them.
+gpue_status step_loop(gpue_ctx* c, int prec, int off, int nsteps, int gstate,
+                      const gpue_evolve_opts& o, bool guard, LoopOut& lo) {
+    const int last = off + nsteps;
+    std::vector<double> rexp;
+    // ramp (src/evolution.cu:409-427): GPUE raises the gauge tables to
+    // omega_0 every step, so the exponent at step i is cumulative
+    if (c->p.ramp && gstate == 0 && gauge_active(c)) {
+        rexp.resize(last);
+        double r = 1.0;
+        for (int i = 0; i < last; ++i) {
+            double w0;
+            if (c->p.ramp_type == 1) w0 = (i == 0) ? c->p.omega : (double)i / (double)(i + 1);
+            else w0 = (i == 0) ? c->p.omega / (double)last : (double)(i + 1) / (double)i;
+            r *= w0;
+            rexp[i] = r;
+        }
+    }
+    const int every = o.energy_calc_steps;
+    const int chunk = o.graph_chunk > 0 ? o.graph_chunk : 64;
+    // GPUE compares with the energy stored by the previous check
+    // (par.dval("energy")), which a sliced run carries across calls
+    double old_energy = off > 0 ? c->last_energy : 0.0;
+    int i = off;
+    bool scale_next = (gstate == 0) && c->pending_scale;
+    while (i < last) {
+        // segments of at most `chunk` steps, ending right after each energy
+        // check step (i % every == 0, as GPUE's evolve checks)
+        int seg_end = i + chunk < last ? i + chunk : last;
+        bool check = false;
+        if (every > 0) {
+            const int nc = ((i + every - 1) / every) * every;
+            if (nc < last && nc + 1 <= seg_end) {
+                seg_end = nc + 1;
+                check = true;
+            }
+        }
+        gpue_status st = run_segment(c, prec, i, seg_end, gstate, scale_next, rexp, check, guard);
+        if (st) return st;
+        if (gstate == 0) {
+            scale_next = true;
+            c->pending_scale = true;
+        }
+        i = seg_end;
+        lo.done = i - off;
+        if (check) {
+            double energy;
+            st = read_energy(c, &energy);
+            if (st) return st;
+            lo.energy = energy;
+            lo.n_en++;
+            c->last_energy = energy;
+            const int step = i - 1;
+            const bool stop =
+                o.threshold_abs ? std::fabs(old_energy - energy) < o.energy_calc_threshold
+                                : std::fabs(old_energy - energy) < o.energy_calc_threshold * old_energy;
+            if (step != 0 && stop && gstate == 0) {
+                lo.early = 1;
+                break;
+            }
+            old_energy = energy;
+        }
+    }
+    return GPUE_OK;
+}
+
+gpue_status ensure_shadow(gpue_ctx* c) {
+    if (c->psi64) return GPUE_OK;
+    CK(cudaMalloc(&c->psi64, c->N * 16));
+    for (int a = 0; a < c->dim; ++a) {
+        gpue_status st = plan_axis(c, GPUE_PREC_FP64, a);
+        if (st) return st;
+    }
+    return GPUE_OK;
+}
+
+// After a polish the FP64 shadow holds the state; bring it back.
+gpue_status unpolish(gpue_ctx* c) {
+    if (!c->polished) return GPUE_OK;
+    k_convert<double, float><<<c->sms * 8, 256, 0, c->stream>>>(c->psi64, c->psi, c->N);
     CK(cudaGetLastError());
-    double h;
-    CK(cudaMemcpyAsync(&h, c->scal + kNorm, sizeof h, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    *out = h * c->dV;
+    c->polished = false;
     return GPUE_OK;
 }
 
@@ -659,7 +782,8 @@ gpue_status gpue_default_params(gpue_params* p) {
     const double N = 1.0;
     p->gDenConst = N * 4 * HBAR * HBAR * kPI * (a_s / mass) *
                    std::sqrt(mass * p->omegaZ / (2 * kPI * HBAR));
-    const double Rxy = std::pow(15.0, 0.2) * std::pow(N * a_s * std::sqrt(mass * p->omegaZ / HBAR), 0.2);
+    const double Rxy =
+        std::pow(15.0, 0.2) * std::pow(N * a_s * std::sqrt(mass * p->omegaZ / HBAR), 0.2);
     const double a0x = std::sqrt(HBAR / (2 * mass * p->omegaX));
     const double a0y = std::sqrt(HBAR / (2 * mass * p->omegaY));
     p->xMax = 6 * Rxy * a0x;
@@ -680,39 +804,39 @@ gpue_status gpue_ctx_create(const gpue_params* p, gpue_ctx** out) {
     c->p = *p;
     c->dim = p->dimnum;
     c->prec = p->precision == GPUE_PREC_FP32 ? GPUE_PREC_FP32 : GPUE_PREC_FP64;
-    if (c->dim != 2 && c->dim != 3)
-        return GPUE_ERR_INVALID_ARG;
+    if (c->dim != 2 && c->dim != 3) return GPUE_ERR_INVALID_ARG;
     const int nx = p->xDim, ny = p->yDim, nz = c->dim == 3 ? p->zDim : 1;
     if (nx < 2 || ny != nx || (c->dim == 3 && nz != nx)) return GPUE_ERR_INVALID_ARG;
     if (!(p->xMax > 0) || !(p->hbar > 0) || !(p->mass > 0)) return GPUE_ERR_INVALID_ARG;
+    if (c->dim > 1 && !(p->yMax > 0)) return GPUE_ERR_INVALID_ARG;
+    if (c->dim > 2 && !(p->zMax > 0)) return GPUE_ERR_INVALID_ARG;
     if (!gpue_supported_length(c->prec, nx)) return GPUE_ERR_UNSUPPORTED;
     build_axis(c->ax[0], nx, p->xMax, true);
-    build_axis(c->ax[1], ny, p->dimnum > 1 ? p->yMax : 1.0, true);
+    build_axis(c->ax[1], ny, p->yMax, true);
     build_axis(c->ax[2], nz, p->zMax, c->dim == 3);
     c->N = (long)nx * ny * nz;
     c->dV = c->ax[0].dx * c->ax[1].dx * (c->dim == 3 ? c->ax[2].dx : 1.0);
     c->device = p->device;
     CK(cudaSetDevice(c->device));
+    CK(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device));
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     CK(cudaEventCreate(&c->ev0));
     CK(cudaEventCreate(&c->ev1));
     CK(cudaMalloc(&c->psi, c->N * elem_size(c->prec)));
     CK(cudaMalloc(&c->scratch, c->N * 16));
     CK(cudaMalloc(&c->scal, kNScal * sizeof(double)));
-    c->partials_cap = c->N / nx + 4096;
+    c->partials_cap = c->N / nx + kAuxPartials + 1024;
     CK(cudaMalloc(&c->partials, c->partials_cap * sizeof(double2)));
     CK(cudaMalloc(&c->counters, kNCtr * sizeof(unsigned)));
     CK(cudaMemsetAsync(c->counters, 0, kNCtr * sizeof(unsigned), c->stream));
-    CK(cudaMemsetAsync(c->scal, 0, kNScal * sizeof(double), c->stream));
+    double hs[kNScal] = {1.0, 0.0, 0.0, 0.0, 1.0, 1.0 / c->dV, 1.0, 1.0};
+    CK(cudaMemcpyAsync(c->scal, hs, sizeof hs, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemsetAsync(c->psi, 0, c->N * elem_size(c->prec), c->stream));
     CK(cudaStreamSynchronize(c->stream));
     gpue_status st = build_tables(c, c->prec, 0);
     if (st) return st;
     for (int a = 0; a < c->dim; ++a) {
-        LaunchCfg lc;
-        st = pass_launch_cfg(c, c->prec, a, lc);
-        if (st) return st;
-        st = set_smem_attr(c, lc, a);
+        st = plan_axis(c, c->prec, a);
         if (st) return st;
     }
     *out = cp.release();
@@ -727,6 +851,7 @@ gpue_status gpue_ctx_destroy(gpue_ctx* c) {
     for (auto& t : c->tab)
         if (t.buf) cudaFree(t.buf);
     cudaFree(c->psi);
+    if (c->psi64) cudaFree(c->psi64);
     cudaFree(c->scratch);
     cudaFree(c->scal);
     cudaFree(c->partials);
@@ -753,21 +878,22 @@ gpue_status gpue_set_wfc(gpue_ctx* c, const void* psi, int32_t mem, int32_t dtyp
     CK(cudaSetDevice(c->device));
     const int want = c->prec == GPUE_PREC_FP32 ? GPUE_C64 : GPUE_C128;
     const size_t in_bytes = c->N * (dtype == GPUE_C128 ? 16 : 8);
-    const cudaMemcpyKind kind = mem == GPUE_MEM_HOST ? cudaMemcpyHostToDevice
-                                                     : cudaMemcpyDeviceToDevice;
+    const cudaMemcpyKind kind =
+        mem == GPUE_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
     if (dtype == want) {
         CK(cudaMemcpyAsync(c->psi, psi, in_bytes, kind, c->stream));
     } else {
         CK(cudaMemcpyAsync(c->scratch, psi, in_bytes, kind, c->stream));
         if (dtype == GPUE_C128)
-            k_convert<double, float><<<148 * 8, 256, 0, c->stream>>>(c->scratch, c->psi, c->N);
+            k_convert<double, float><<<c->sms * 8, 256, 0, c->stream>>>(c->scratch, c->psi, c->N);
         else
-            k_convert<float, double><<<148 * 8, 256, 0, c->stream>>>(c->scratch, c->psi, c->N);
+            k_convert<float, double><<<c->sms * 8, 256, 0, c->stream>>>(c->scratch, c->psi, c->N);
         CK(cudaGetLastError());
     }
     CK(cudaStreamSynchronize(c->stream));
     c->have_wfc = true;
     c->pending_scale = false;
+    c->polished = false;
     return GPUE_OK;
 }
 
@@ -776,19 +902,21 @@ gpue_status gpue_get_wfc(gpue_ctx* c, void* psi, int32_t mem, int32_t dtype) {
         (dtype != GPUE_C128 && dtype != GPUE_C64))
         return GPUE_ERR_INVALID_ARG;
     CK(cudaSetDevice(c->device));
-    gpue_status st = apply_pending_scale(c);
+    const int sp = c->polished ? GPUE_PREC_FP64 : c->prec;
+    gpue_status st = apply_pending_scale(c, sp);
     if (st) return st;
-    const int have = c->prec == GPUE_PREC_FP32 ? GPUE_C64 : GPUE_C128;
+    void* src = state_of(c, sp);
+    const int have = sp == GPUE_PREC_FP32 ? GPUE_C64 : GPUE_C128;
     const size_t out_bytes = c->N * (dtype == GPUE_C128 ? 16 : 8);
-    const cudaMemcpyKind kind = mem == GPUE_MEM_HOST ? cudaMemcpyDeviceToHost
-                                                     : cudaMemcpyDeviceToDevice;
+    const cudaMemcpyKind kind =
+        mem == GPUE_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     if (dtype == have) {
-        CK(cudaMemcpyAsync(psi, c->psi, out_bytes, kind, c->stream));
+        CK(cudaMemcpyAsync(psi, src, out_bytes, kind, c->stream));
     } else {
         if (have == GPUE_C64)
-            k_convert<float, double><<<148 * 8, 256, 0, c->stream>>>(c->psi, c->scratch, c->N);
+            k_convert<float, double><<<c->sms * 8, 256, 0, c->stream>>>(src, c->scratch, c->N);
         else
-            k_convert<double, float><<<148 * 8, 256, 0, c->stream>>>(c->psi, c->scratch, c->N);
+            k_convert<double, float><<<c->sms * 8, 256, 0, c->stream>>>(src, c->scratch, c->N);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(psi, c->scratch, out_bytes, kind, c->stream));
     }
@@ -800,8 +928,11 @@ gpue_status gpue_energy(gpue_ctx* c, double* E) {
     if (!c || !E) return GPUE_ERR_INVALID_ARG;
     if (!c->have_wfc) return fail(c, GPUE_ERR_STATE, "no wavefunction set");
     CK(cudaSetDevice(c->device));
-    const int gs = c->tab[c->prec].built_for < 0 ? 0 : c->tab[c->prec].built_for;
-    gpue_status st = launch_energy(c, c->prec, gs, c->pending_scale);
+    const int sp = c->polished ? GPUE_PREC_FP64 : c->prec;
+    const int gs = c->tab[sp].built_for < 0 ? 0 : c->tab[sp].built_for;
+    gpue_status st = build_tables(c, sp, gs);
+    if (st) return st;
+    st = launch_energy(c, sp, gs, c->pending_scale);
     if (st) return st;
     return read_energy(c, E);
 }
@@ -809,9 +940,10 @@ gpue_status gpue_energy(gpue_ctx* c, double* E) {
 gpue_status gpue_norm(gpue_ctx* c, double* out) {
     if (!c || !out) return GPUE_ERR_INVALID_ARG;
     CK(cudaSetDevice(c->device));
-    gpue_status st = apply_pending_scale(c);
+    const int sp = c->polished ? GPUE_PREC_FP64 : c->prec;
+    gpue_status st = apply_pending_scale(c, sp);
     if (st) return st;
-    return norm_now(c, out);
+    return norm_now(c, sp, out);
 }
 
 gpue_status gpue_ctx_stream(gpue_ctx* c, void** s) {
@@ -834,82 +966,59 @@ gpue_status gpue_evolve(gpue_ctx* c, int32_t nsteps, int32_t gstate,
     CK(cudaSetDevice(c->device));
     gpue_evolve_opts o;
     std::memset(&o, 0, sizeof o);
+    o.norm_guard = -1;
     if (opts) o = *opts;
-    if (o.polish_steps > 0 && c->prec == GPUE_PREC_FP64) o.polish_steps = 0;
+    if (o.polish_steps < 0 || o.graph_chunk < 0 || o.step_offset < 0)
+        return GPUE_ERR_INVALID_ARG;
     if (o.no_sync && o.energy_calc_steps > 0)
         return fail(c, GPUE_ERR_INVALID_ARG, "no_sync excludes energy checks");
-    gpue_status st = build_tables(c, c->prec, gstate);
+    const bool polish = o.polish_steps > 0 && c->prec == GPUE_PREC_FP32 && gstate == 0;
+    const bool guard = gstate == 1 && (o.norm_guard == 1 ||
+                                       (o.norm_guard < 0 && c->prec == GPUE_PREC_FP32));
+    gpue_status st = unpolish(c);
+    if (st) return st;
+    st = build_tables(c, c->prec, gstate);
     if (st) return st;
     c->launches = 0;
-    // ramp exponent per step (src/evolution.cu:409-427): GPUE raises the gauge
-    // tables to omega_0 every step, so the exponent at step i is cumulative
-    // absolute step indices [off, last): time = Dt*i and the gauge order i%2
-    const int off = o.step_offset > 0 ? o.step_offset : 0;
-    const int last = off + nsteps;
-    std::vector<double> rexp;
-    if (c->p.ramp && gstate == 0 && gauge_active(c)) {
-        rexp.resize(last);
-        double r = 1.0;
-        for (int i = 0; i < last; ++i) {
-            double w0;
-            if (c->p.ramp_type == 1) w0 = (i == 0) ? c->p.omega : (double)i / (double)(i + 1);
-            else w0 = (i == 0) ? c->p.omega / (double)last : (double)(i + 1) / (double)i;
-            r *= w0;
-            rexp[i] = r;
-        }
-    }
-    const int every = o.energy_calc_steps;
-    const int chunk = o.graph_chunk > 0 ? o.graph_chunk : 64;
+    const int off = o.step_offset;
     CK(cudaEventRecord(c->ev0, c->stream));
-    // GPUE compares with the energy stored by the previous check
-    // (par.dval("energy")), which a sliced run carries across calls
-    double old_energy = off > 0 ? c->last_energy : 0.0, energy = NAN;
-    int n_en = 0, done = 0, early = 0;
-    int i = off;
-    // the first imaginary step has no deferred scale to apply
-    bool scale_next = (gstate == 0) && c->pending_scale;
-    while (i < last) {
-        // segments of at most `chunk` steps, ending right after each energy
-        // check step (i % every == 0, as GPUE's evolve checks)
-        int seg_end = i + chunk < last ? i + chunk : last;
-        bool check = false;
-        if (every > 0) {
-            const int nc = ((i + every - 1) / every) * every;
-            if (nc < last && nc + 1 <= seg_end) {
-                seg_end = nc + 1;
-                check = true;
-            }
-        }
-        st = run_segment(c, i, seg_end, gstate, scale_next, rexp, check, true);
+    if (guard) {
+        st = norm_to_slot(c, c->prec, kTargetReal);
         if (st) return st;
-        if (gstate == 0) {
-            scale_next = true;
-            c->pending_scale = true;
-        }
-        i = seg_end;
-        done = i - off;
-        if (check) {
-            st = read_energy(c, &energy);
-            if (st) return st;
-            n_en++;
-            c->last_energy = energy;
-            const int step = i - 1;
-            bool stop = o.threshold_abs
-                            ? std::fabs(old_energy - energy) < o.energy_calc_threshold
-                            : std::fabs(old_energy - energy) < o.energy_calc_threshold * old_energy;
-            if (step != 0 && stop && gstate == 0) {
-                early = 1;
-                break;
-            }
-            old_energy = energy;
-        }
+        CK(cudaMemcpyAsync(c->scal + kGuard, c->scal + kOne, sizeof(double),
+                           cudaMemcpyDeviceToDevice, c->stream));
     }
-    st = apply_pending_scale(c);
+    LoopOut lo;
+    st = step_loop(c, c->prec, off, nsteps, gstate, o, guard, lo);
     if (st) return st;
+    st = apply_pending_scale(c, c->prec);
+    if (st) return st;
+    if (guard) {
+        st = scale_state(c, c->prec, kGuard);
+        if (st) return st;
+    }
+    if (polish) {
+        // FP64 polishing steps that continue the imaginary-time run
+        st = ensure_shadow(c);
+        if (st) return st;
+        st = build_tables(c, GPUE_PREC_FP64, 0);
+        if (st) return st;
+        k_convert<float, double><<<c->sms * 8, 256, 0, c->stream>>>(c->psi, c->psi64, c->N);
+        CK(cudaGetLastError());
+        gpue_evolve_opts po = o;
+        po.energy_calc_steps = 0;
+        LoopOut pl;
+        st = step_loop(c, GPUE_PREC_FP64, off + lo.done, o.polish_steps, 0, po, false, pl);
+        if (st) return st;
+        st = apply_pending_scale(c, GPUE_PREC_FP64);
+        if (st) return st;
+        c->polished = true;
+        lo.done += pl.done;
+    }
     if (o.no_sync) {
         if (res) {
             std::memset(res, 0, sizeof *res);
-            res->steps_done = done;
+            res->steps_done = lo.done;
             res->energy = NAN;
             res->kernel_launches = c->launches;
         }
@@ -921,14 +1030,14 @@ gpue_status gpue_evolve(gpue_ctx* c, int32_t nsteps, int32_t gstate,
     CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
     if (res) {
         std::memset(res, 0, sizeof *res);
-        res->steps_done = done;
-        res->early_stop = early;
-        res->n_energies = n_en;
-        res->energy = energy;
+        res->steps_done = lo.done;
+        res->early_stop = lo.early;
+        res->n_energies = lo.n_en;
+        res->energy = lo.energy;
         res->device_ms = ms;
         res->kernel_launches = c->launches;
         double nrm = 0;
-        st = norm_now(c, &nrm);
+        st = norm_now(c, c->polished ? GPUE_PREC_FP64 : c->prec, &nrm);
         if (st) return st;
         res->norm = nrm;
     }

@@ -14,14 +14,17 @@
 //
 // Stage 0 reads straight from the registers loaded from HBM, the last stage
 // leaves its outputs in registers, and the middle exchanges go through shared
-// memory.  Because the sequence is palindromic, the register layout before and
-// after a transform is the same ("layout D": register e = q*RA + r holds
-// element t + P*q + r*N/RA), so forward and inverse transforms and pointwise
-// phase multiplies chain inside one kernel without extra data movement, and
-// global loads/stores in layout D are coalesced across threads.
+// memory (one 8- or 16-byte access per element).  Because the sequence is
+// palindromic, the register layout before and after a transform is the same
+// ("layout D": register e = q*RA + r holds element t + P*q + r*N/RA), so
+// forward and inverse transforms and pointwise phase multiplies chain inside
+// one kernel without extra data movement, and global loads/stores in layout D
+// are coalesced across threads.
 //
-// The unnormalised DFT convention is cuFFT's (forward exp(-2 pi i jk/N),
-// inverse exp(+2 pi i jk/N)), which is what GPUE's evolve() uses.
+// Transforms are unnormalised with cuFFT's signs (forward exp(-2 pi i jk/N)),
+// which is what GPUE's evolve() uses before its 1/sqrt(N) scalarMult; the
+// passes fold the 1/N of each forward/inverse pair into a phase factor.  The
+// inverse is conj(F(conj(x))), so one FFT body serves both directions.
 
 #pragma once
 
@@ -51,16 +54,12 @@ template <typename T>
 __device__ __forceinline__ cx<T> cscale(cx<T> a, T s) { return {a.x * s, a.y * s}; }
 template <typename T>
 __device__ __forceinline__ cx<T> cconj(cx<T> a) { return {a.x, -a.y}; }
-// multiply by -i (forward) or +i (inverse)
-template <bool INV, typename T>
-__device__ __forceinline__ cx<T> mul_mi(cx<T> a) {
-    if constexpr (INV) return {-a.y, a.x};
-    else return {a.y, -a.x};
-}
+// multiply by -i
+template <typename T>
+__device__ __forceinline__ cx<T> mul_mi(cx<T> a) { return {a.y, -a.x}; }
 
-// a * W_R^m with W_R = exp(-2 pi i / R) (forward) or its conjugate (inverse);
-// exact shortcuts for the multiples of pi/2 and pi/4.
-template <int R, int M, bool INV, typename T>
+// a * W_R^m, W_R = exp(-2 pi i / R), with exact shortcuts at multiples of pi/4
+template <int R, int M, typename T>
 __device__ __forceinline__ cx<T> tw_const(cx<T> a) {
     constexpr int m = ((M % R) + R) % R;
     if constexpr (m == 0) {
@@ -68,32 +67,31 @@ __device__ __forceinline__ cx<T> tw_const(cx<T> a) {
     } else if constexpr (2 * m == R) {
         return {-a.x, -a.y};
     } else if constexpr (4 * m == R) {
-        return mul_mi<INV>(a);
+        return mul_mi(a);
     } else if constexpr (4 * m == 3 * R) {
-        return mul_mi<!INV>(a);
+        return {-a.y, a.x};
     } else if constexpr (8 * m == R || 8 * m == 3 * R || 8 * m == 5 * R || 8 * m == 7 * R) {
         constexpr T h = (T)0.70710678118654752440;
         constexpr double c = tw_cos(R, m);
         constexpr double s = tw_sin(R, m);
-        // (c - i s) for forward, (c + i s) inverse; |c| = |s| = h
         constexpr T cs = c > 0 ? h : -h;
-        constexpr T ss = INV ? (s > 0 ? h : -h) : (s > 0 ? -h : h);
+        constexpr T ss = s > 0 ? -h : h;  // W = c - i s
         return {cs * a.x - ss * a.y, cs * a.y + ss * a.x};
     } else {
         constexpr T c = (T)tw_cos(R, m);
-        constexpr T s = INV ? (T)tw_sin(R, m) : (T)-tw_sin(R, m);
+        constexpr T s = (T)-tw_sin(R, m);
         return {c * a.x - s * a.y, c * a.y + s * a.x};
     }
 }
 
 // ---------------------------------------------------------- small DFTs --
-// In-place R-point DFT of v[0..R-1] in registers, natural-order output.
+// In-place forward R-point DFT of v[0..R-1] in registers, natural order.
 
-template <int R, bool INV, typename T>
+template <int R, typename T>
 struct SmallDFT;
 
-template <bool INV, typename T>
-struct SmallDFT<2, INV, T> {
+template <typename T>
+struct SmallDFT<2, T> {
     static __device__ __forceinline__ void run(cx<T>* v) {
         cx<T> a = v[0], b = v[1];
         v[0] = a + b;
@@ -101,11 +99,11 @@ struct SmallDFT<2, INV, T> {
     }
 };
 
-template <bool INV, typename T>
-struct SmallDFT<3, INV, T> {
+template <typename T>
+struct SmallDFT<3, T> {
     static __device__ __forceinline__ void run(cx<T>* v) {
         constexpr T c1 = (T)-0.5;
-        constexpr T s1 = INV ? (T)tw_sin(3, 1) : (T)-tw_sin(3, 1);
+        constexpr T s1 = (T)-tw_sin(3, 1);
         cx<T> t1 = v[1] + v[2];
         cx<T> t2 = v[1] - v[2];
         cx<T> a = {v[0].x + c1 * t1.x, v[0].y + c1 * t1.y};
@@ -116,11 +114,11 @@ struct SmallDFT<3, INV, T> {
     }
 };
 
-template <bool INV, typename T>
-struct SmallDFT<4, INV, T> {
+template <typename T>
+struct SmallDFT<4, T> {
     static __device__ __forceinline__ void run(cx<T>* v) {
         cx<T> s02 = v[0] + v[2], d02 = v[0] - v[2];
-        cx<T> s13 = v[1] + v[3], d13 = mul_mi<INV>(v[1] - v[3]);
+        cx<T> s13 = v[1] + v[3], d13 = mul_mi(v[1] - v[3]);
         v[0] = s02 + s13;
         v[1] = d02 + d13;
         v[2] = s02 - s13;
@@ -128,12 +126,12 @@ struct SmallDFT<4, INV, T> {
     }
 };
 
-template <bool INV, typename T>
-struct SmallDFT<5, INV, T> {
+template <typename T>
+struct SmallDFT<5, T> {
     static __device__ __forceinline__ void run(cx<T>* v) {
         constexpr T c1 = (T)tw_cos(5, 1), c2 = (T)tw_cos(5, 2);
-        constexpr T s1 = INV ? (T)tw_sin(5, 1) : (T)-tw_sin(5, 1);
-        constexpr T s2 = INV ? (T)tw_sin(5, 2) : (T)-tw_sin(5, 2);
+        constexpr T s1 = (T)-tw_sin(5, 1);
+        constexpr T s2 = (T)-tw_sin(5, 2);
         cx<T> a1 = v[1] + v[4], b1 = v[1] - v[4];
         cx<T> a2 = v[2] + v[3], b2 = v[2] - v[3];
         cx<T> r1 = {v[0].x + c1 * a1.x + c2 * a2.x, v[0].y + c1 * a1.y + c2 * a2.y};
@@ -149,9 +147,8 @@ struct SmallDFT<5, INV, T> {
     }
 };
 
-// Composite R = A*B (A the smallest prime-power factor handled directly):
-// B DFTs of length A on stride-B subsequences, twiddles W_R^{b k1}, then A
-// DFTs of length B; X[k1 + A*k2].
+// Composite R = A*B: B DFTs of length A on stride-B subsequences, twiddles
+// W_R^{b k1}, then A DFTs of length B; X[k1 + A*k2].
 template <int R>
 struct Split {
     static constexpr int A = (R % 4 == 0 && R != 8 && R != 4) ? 4
@@ -161,13 +158,18 @@ struct Split {
     static constexpr int B = R / A;
 };
 
-template <int R, bool INV, typename T>
+template <int R, typename T>
 struct SmallDFT {
     static constexpr int A = Split<R>::A;
     static constexpr int B = Split<R>::B;
     template <int b, int k1>
     static __device__ __forceinline__ void tw_one(cx<T> (&y)[B][A]) {
-        y[b][k1] = tw_const<R, b * k1, INV>(y[b][k1]);
+        y[b][k1] = tw_const<R, b * k1>(y[b][k1]);
+    }
+    template <int... I>
+    static __device__ __forceinline__ void twiddle_all(cx<T> (&y)[B][A],
+                                                       std::integer_sequence<int, I...>) {
+        (tw_one<I / A, I % A>(y), ...);
     }
     static __device__ __forceinline__ void run(cx<T>* v) {
         cx<T> y[B][A];
@@ -175,7 +177,7 @@ struct SmallDFT {
         for (int b = 0; b < B; ++b) {
 #pragma unroll
             for (int a = 0; a < A; ++a) y[b][a] = v[b + B * a];
-            SmallDFT<A, INV, T>::run(y[b]);
+            SmallDFT<A, T>::run(y[b]);
         }
         twiddle_all(y, std::make_integer_sequence<int, B * A>{});
         cx<T> z[B];
@@ -183,21 +185,16 @@ struct SmallDFT {
         for (int k1 = 0; k1 < A; ++k1) {
 #pragma unroll
             for (int b = 0; b < B; ++b) z[b] = y[b][k1];
-            SmallDFT<B, INV, T>::run(z);
+            SmallDFT<B, T>::run(z);
 #pragma unroll
             for (int k2 = 0; k2 < B; ++k2) v[k1 + A * k2] = z[k2];
         }
-    }
-    template <int... I>
-    static __device__ __forceinline__ void twiddle_all(cx<T> (&y)[B][A],
-                                                       std::integer_sequence<int, I...>) {
-        (tw_one<I / A, I % A>(y), ...);
     }
 };
 
 // ------------------------------------------------------------ line FFT --
 
-__device__ __forceinline__ int smem_phys(int i) { return i + (i >> 5); }
+__host__ __device__ __forceinline__ constexpr int smem_phys(int i) { return i + (i >> 4); }
 
 template <typename T, int N_, int RA, int RB, int P_>
 struct LineFFT {
@@ -208,19 +205,22 @@ struct LineFFT {
     static_assert(NS == 2 ? N == RA * RA : N == RA * RB * RA, "palindromic radix plan");
     static_assert((N / RA) % P == 0, "threads must divide the butterflies of the outer stages");
     static_assert(NS == 2 || (N / RB) % P == 0, "threads must divide the middle stage");
-    // smem line stride (elements of T per re/im array): one pad per 32, plus a
-    // bank offset so lines that share a warp land on different banks
-    static constexpr int LS = N + N / 32 + 8;
+    // smem line stride in complex elements: one pad per 16, rounded to 16 and
+    // offset by 4 so the lines a strided-pass warp touches (lanes c + C*t)
+    // fall on distinct banks
+    static constexpr int LS = ((smem_phys(N - 1) + 1 + 15) / 16) * 16 + 4;
 
     __host__ __device__ static constexpr int radix(int s) { return (NS == 3 && s == 1) ? RB : RA; }
-    __host__ __device__ static constexpr int ns_before(int s) { return s == 0 ? 1 : s == 1 ? RA : RA * RB; }
+    __host__ __device__ static constexpr int ns_before(int s) {
+        return s == 0 ? 1 : s == 1 ? RA : RA * RB;
+    }
 
     // element index held by register e in layout D
     static __device__ __forceinline__ int index(int t, int e) {
         return t + P * (e / RA) + (e % RA) * (N / RA);
     }
 
-    template <int S, bool INV>
+    template <int S>
     static __device__ __forceinline__ void compute(cx<T> (&v)[E], int t,
                                                    const cx<T>* __restrict__ tw) {
         constexpr int R = radix(S);
@@ -233,20 +233,15 @@ struct LineFFT {
                 const int jm = j % Ns;
                 constexpr int step = N / (Ns * R);
 #pragma unroll
-                for (int r = 1; r < R; ++r) {
-                    cx<T> w = tw[jm * r * step];
-                    if constexpr (INV) w.y = -w.y;
-                    v[q * R + r] = cmul(v[q * R + r], w);
-                }
+                for (int r = 1; r < R; ++r) v[q * R + r] = cmul(v[q * R + r], tw[jm * r * step]);
             }
-            SmallDFT<R, INV, T>::run(&v[q * R]);
+            SmallDFT<R, T>::run(&v[q * R]);
         }
     }
 
     // Write stage S's outputs to smem, sync, read stage S+1's inputs, sync.
     template <int S, typename Sync>
-    static __device__ __forceinline__ void exchange(cx<T> (&v)[E], int t, T* sre, T* sim,
-                                                    Sync sync) {
+    static __device__ __forceinline__ void exchange(cx<T> (&v)[E], int t, cx<T>* sl, Sync sync) {
         constexpr int R = radix(S);
         constexpr int Ns = ns_before(S);
         constexpr int G = N / (R * P);
@@ -255,11 +250,7 @@ struct LineFFT {
             const int j = t + P * q;
             const int base = (j / Ns) * Ns * R + (j % Ns);
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int p = smem_phys(base + r * Ns);
-                sre[p] = v[q * R + r].x;
-                sim[p] = v[q * R + r].y;
-            }
+            for (int r = 0; r < R; ++r) sl[smem_phys(base + r * Ns)] = v[q * R + r];
         }
         sync();
         constexpr int R2 = radix(S + 1);
@@ -268,23 +259,21 @@ struct LineFFT {
         for (int q = 0; q < G2; ++q) {
             const int j = t + P * q;
 #pragma unroll
-            for (int r = 0; r < R2; ++r) {
-                const int p = smem_phys(j + r * (N / R2));
-                v[q * R2 + r] = cx<T>{sre[p], sim[p]};
-            }
+            for (int r = 0; r < R2; ++r) v[q * R2 + r] = sl[smem_phys(j + r * (N / R2))];
         }
         sync();
     }
 
-    template <bool INV, typename Sync>
-    static __device__ __forceinline__ void run(cx<T> (&v)[E], int t, T* sre, T* sim,
-                                               const cx<T>* __restrict__ tw, Sync sync) {
-        compute<0, INV>(v, t, tw);
-        exchange<0>(v, t, sre, sim, sync);
-        compute<1, INV>(v, t, tw);
+    // Unnormalised forward DFT of the line (inverse: conjugate around it).
+    template <typename Sync>
+    static __device__ __forceinline__ void forward(cx<T> (&v)[E], int t, cx<T>* sl,
+                                                   const cx<T>* __restrict__ tw, Sync sync) {
+        compute<0>(v, t, tw);
+        exchange<0>(v, t, sl, sync);
+        compute<1>(v, t, tw);
         if constexpr (NS == 3) {
-            exchange<1>(v, t, sre, sim, sync);
-            compute<2, INV>(v, t, tw);
+            exchange<1>(v, t, sl, sync);
+            compute<2>(v, t, tw);
         }
     }
 };

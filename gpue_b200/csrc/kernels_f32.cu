@@ -1,4 +1,8 @@
 // kernels_f32.cu -- complex64 pass kernels (the fused FP32 form).
+//
+// One plan per line length: radix sequence (RA, RA) or (RA, RB, RA) and P
+// threads per line, chosen for E = N/P <= 16 complex values per thread where
+// the length allows it (more resident warps, shorter straight-line code).
 #include "registry.h"
 
 namespace gpue {
@@ -10,18 +14,18 @@ namespace gpue {
 static const PassKernel kTableF32[] = {
     GPUE_PLAN(float, 16, 4, 0, 4),
     GPUE_PLAN(float, 32, 4, 2, 8),
-    GPUE_PLAN(float, 64, 8, 0, 8),
+    GPUE_PLAN(float, 64, 4, 4, 16),
     GPUE_PLAN(float, 96, 4, 6, 8),
-    GPUE_PLAN(float, 128, 8, 2, 16),
+    GPUE_PLAN(float, 128, 4, 8, 16),
     GPUE_PLAN(float, 160, 4, 10, 8),
     GPUE_PLAN(float, 192, 4, 12, 16),
-    GPUE_PLAN(float, 256, 16, 0, 16),
+    GPUE_PLAN(float, 256, 8, 4, 32),
     GPUE_PLAN(float, 320, 4, 20, 16),
     GPUE_PLAN(float, 384, 4, 24, 16),
-    GPUE_PLAN(float, 512, 8, 8, 32),
+    GPUE_PLAN(float, 512, 8, 8, 64),
     GPUE_PLAN(float, 640, 8, 10, 16),
     GPUE_PLAN(float, 768, 8, 12, 32),
-    GPUE_PLAN(float, 1024, 32, 0, 32),
+    GPUE_PLAN(float, 1024, 16, 4, 64),
 };
 
 const PassKernel* pass_table_f32(int* count) {

@@ -1,34 +1,38 @@
 // pass.cuh -- one full-field read+write pass over lines of one axis.
 //
-// A pass loads C lines per CTA (rows for axis 0; C adjacent columns for the
-// strided axes 1 and 2, so every row segment is one 32-byte sector for
-// complex64), runs a short program of operations on the registers, and stores
-// the lines back.  The operations are the pieces of GPUE's split step
-// (src/evolution.cu:727-870), fused so each pass touches HBM once:
+// A pass walks tiles of C lines (rows for axis 0; C adjacent columns for the
+// strided axes 1 and 2, so each row segment is at least one 32-byte sector),
+// loads a tile into registers, runs a short program of operations, and
+// stores it back.  The operations are the pieces of GPUE's split step
+// (src/evolution.cu:727-870), fused so each pass touches memory once:
 //
-//   OP_SCALE   psi *= pending renormalisation 1/sqrt(sum|psi|^2 dV)
-//              (parSum/scalarDiv_wfcNorm, src/split_op.cu:83-129, deferred to
-//              the next pass that reads the field)
+//   OP_SCALE   psi *= deferred renormalisation factor (parSum and
+//              scalarDiv_wfcNorm, src/split_op.cu:83-129, applied by the next
+//              pass that reads the field)
 //   OP_VHALF   psi *= exp(-(V + gN|psi|^2) Dt/(2 hbar))        imaginary time
 //              psi *= exp(-i(V + gN|psi|^2) Dt/(2 hbar))       real time
-//              (cMultDensity, src/kernels.cu:365-388; linear form cMult)
-//   OP_FFT_F / OP_FFT_I   1D DFT along the pass axis, times 1/sqrt(n)
-//              (cufftExecZ2Z + scalarMult, src/evolution.cu:758-777)
-//   OP_KPHASE  psi *= exp(-K Dt/hbar) / exp(-i K Dt/hbar),
-//              K = hbar^2/(2m) |p|^2 (src/operators.cu:460-469, 1081-1103)
-//   OP_GAUGE   psi *= exp(-A_a p_a gdt) / exp(-i A_a p_a dt) along the pass
-//              axis (apply_gauge, src/evolution.cu:5-257; aux_fields
+//              (cMultDensity, src/kernels.cu:365-388; cMult without -s)
+//   OP_FFT_F / OP_FFT_I   unnormalised 1D DFT along the pass axis
+//              (cufftExecZ2Z, src/evolution.cu:758,774)
+//   OP_KPHASE  psi *= exp(-K Dt/hbar) / exp(-i K Dt/hbar) times 1/N, the
+//              product of GPUE's two 1/sqrt(N) scalarMults
+//              (K = hbar^2/(2m)|p|^2, src/operators.cu:460-469, 1081-1103)
+//   OP_GAUGE   psi *= exp(-A_a p_a gdt) / exp(-i A_a p_a dt) times 1/n along
+//              the pass axis (apply_gauge, src/evolution.cu:5-257; aux_fields
 //              src/operators.cu:1089-1110)
-//   OP_NORM    accumulate sum |psi|^2 (FP64, compensated) -> renorm scale
+//   OP_NORM    accumulate sum |psi|^2 (FP64, compensated) -> renorm factor
 //   OP_EKIN    accumulate sum K |psi_k|^2 (FP64, compensated)
 //
-// V, K and the imaginary/real-time factors are separable per axis for the
-// harmonic trap with the rotation gauge (V = Vx(x) + Vy(y) + Vz(z) including
-// m|A|^2/2), so the factors come from small per-axis tables computed in FP64
-// on the host (rounded to FP32 for the complex64 form); the nonlinear and
-// gauge phases are evaluated per point.
+// V and K are separable per axis for the harmonic trap with the rotation
+// gauge (V = Vx(x)+Vy(y)+Vz(z) including m|A|^2/2), so their factors come from
+// per-axis FP64 tables.  Every phase factor is formed and applied in FP64 and
+// real-time factors are normalised to unit modulus before the product is
+// rounded back to the storage type: a complex64 factor rounded once and
+// reused every step would otherwise grow or shrink the norm systematically.
 
 #pragma once
+
+#include <type_traits>
 
 #include "fft_core.cuh"
 
@@ -53,11 +57,11 @@ enum RedKind : int { RED_NONE = 0, RED_NORM = 1, RED_SUM = 2 };
 // A grid-wide FP64 reduction: every CTA writes a compensated partial, the last
 // CTA to finish sums them in index order and writes the result.
 struct RedArgs {
-    int kind;           // RED_NONE / RED_NORM (writes 1/sqrt(sum dV)) / RED_SUM
-    double2* partials;  // [gridDim.x] (sum, compensation)
-    unsigned* counter;  // zero between reductions; reset by the last CTA
-    double* out;
-    double dV;
+    int kind;               // RED_NONE / RED_NORM / RED_SUM
+    double2* partials;      // [gridDim.x] (sum, compensation)
+    unsigned* counter;      // zero between reductions; reset by the last CTA
+    double* out;            // RED_NORM: sqrt(*target / sum); RED_SUM: sum
+    const double* target;   // RED_NORM target sum |psi|^2
 };
 
 struct PassArgs {
@@ -65,24 +69,28 @@ struct PassArgs {
     void* out;
     int axis;  // 0: x rows (contiguous), 1: y lines (stride nx), 2: z lines
     int nx, ny, nz;
+    long ntiles;  // tiles of C lines
     int nops;
     int ops[kMaxOps];
     int store;   // write the lines back
     int gstate;  // 0 imaginary time, 1 real time
     int gpe;     // nonlinear term on
     double nl_coef;     // gN * (Dt/2) / hbar
+    double kscale;      // folded into OP_KPHASE (1/N)
+    double gscale;      // folded into OP_GAUGE (1/n of this axis)
     double gauge_coef;  // A_axis = gauge_coef * pos[gauge_src][.]
     int gauge_src;      // axis whose coordinate A_axis depends on
     double gauge_dt;    // gdt * ramp exponent (imaginary) or dt (real)
+    double dmom;        // momentum spacing dp of the pass axis
     double kin_coef;    // hbar^2 / (2 m), for OP_EKIN
-    const void* vfac[3];  // cx<T>[n_a]: per-axis V half-step factor
-    const void* kfac[3];  // cx<T>[n_a]: per-axis kinetic factor
+    const double2* vfac[3];  // per-axis V half-step factor (FP64)
+    const double2* kfac[3];  // per-axis kinetic factor (FP64)
     const double* pos[3];
     const double* mom[3];
     const void* tw;  // cx<T>[N]: W_N^k for this axis
-    double inv_sqrt_n;
     RedArgs red;
-    const double* scale_in;  // OP_SCALE factor
+    const double* scale_in;   // OP_SCALE factor
+    const double* kscale_in;  // optional extra OP_KPHASE factor (real-time norm guard)
 };
 
 // ------------------------------------------------------- FP64 reductions --
@@ -110,7 +118,7 @@ struct KSum {
 };
 
 // Block-wide compensated reduction; result valid in thread 0.  `scratch`
-// needs 2*(blockDim/32) doubles and must not be in use by other threads.
+// needs 2*(blockDim/32) doubles.
 __device__ __forceinline__ KSum block_reduce(KSum k, double* scratch) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -133,8 +141,7 @@ __device__ __forceinline__ KSum block_reduce(KSum k, double* scratch) {
 }
 
 // Write this block's partial; the last block to arrive reduces all partials in
-// index order (deterministic) and writes the result.  Must be called by all
-// threads of the block.
+// index order (deterministic) and writes the result.  All threads call it.
 __device__ __forceinline__ void grid_reduce_finish(KSum k, double* scratch, const RedArgs& a) {
     __shared__ unsigned s_last;
     k = block_reduce(k, scratch);
@@ -157,7 +164,7 @@ __device__ __forceinline__ void grid_reduce_finish(KSum k, double* scratch, cons
         if (threadIdx.x == 0) {
             double sum = t.s + t.c;
             if (a.kind == RED_NORM)
-                a.out[0] = 1.0 / sqrt(sum * a.dV);
+                a.out[0] = sqrt(*a.target / sum);
             else
                 a.out[0] = sum;
             *a.counter = 0u;
@@ -167,27 +174,94 @@ __device__ __forceinline__ void grid_reduce_finish(KSum k, double* scratch, cons
 
 // ------------------------------------------------------------- helpers --
 
-template <typename T>
-__device__ __forceinline__ cx<T> ldc(const void* p, int i) {
-    return reinterpret_cast<const cx<T>*>(p)[i];
+__device__ __forceinline__ cx<double> ld2(const double2* p, int i) {
+    const double2 v = p[i];
+    return {v.x, v.y};
 }
 
-__device__ __forceinline__ void sincos_t(double a, double* s, double* c) { sincos(a, s, c); }
-__device__ __forceinline__ void sincos_t(float a, float* s, float* c) { sincosf(a, s, c); }
-__device__ __forceinline__ double exp_t(double a) { return exp(a); }
-__device__ __forceinline__ float exp_t(float a) { return expf(a); }
+// psi * f with f in FP64; for complex64 the product is formed in FP64 and
+// rounded once.
+template <typename T>
+__device__ __forceinline__ cx<T> apply(cx<T> v, cx<double> f) {
+    if constexpr (std::is_same<T, double>::value) {
+        return cmul(v, f);
+    } else {
+        const double x = v.x, y = v.y;
+        return cx<T>{(T)(x * f.x - y * f.y), (T)(x * f.y + y * f.x)};
+    }
+}
+
+// exp(-i a) for 0 <= a < 1/16 by its Taylor series (truncation error below
+// a^9/9! < 4e-17), else by sincos; |result| = 1 to FP64 accuracy.
+template <typename T>
+__device__ __forceinline__ cx<double> unit_phase(double a);
+
+template <typename T>
+__device__ __forceinline__ cx<double> small_phase(double a) {
+    if (fabs(a) < 0.0625) {
+        const double a2 = a * a;
+        const double s = a * (1.0 - a2 * (1.0 / 6.0 - a2 * (1.0 / 120.0 - a2 * (1.0 / 5040.0))));
+        const double c =
+            1.0 - a2 * (0.5 - a2 * (1.0 / 24.0 - a2 * (1.0 / 720.0 - a2 * (1.0 / 40320.0))));
+        return {c, -s};
+    }
+    return unit_phase<T>(a);
+}
+
+// exp(-a) for 0 <= a < 1/16 by its Taylor series (truncation error below
+// a^10/10! < 5e-19), else by exp.
+template <typename T>
+__device__ __forceinline__ double decay(double a);
+
+template <typename T>
+__device__ __forceinline__ double small_decay(double a) {
+    if (fabs(a) < 0.0625) {
+        double r = 1.0 / 362880.0;
+        r = 1.0 / 40320.0 - a * r;
+        r = 1.0 / 5040.0 - a * r;
+        r = 1.0 / 720.0 - a * r;
+        r = 1.0 / 120.0 - a * r;
+        r = 1.0 / 24.0 - a * r;
+        r = 1.0 / 6.0 - a * r;
+        r = 0.5 - a * r;
+        r = 1.0 - a * r;
+        return 1.0 - a * r;
+    }
+    return decay<T>(a);
+}
+
+// exp(-i a) with unit modulus to FP64 accuracy
+template <typename T>
+__device__ __forceinline__ cx<double> unit_phase(double a) {
+    if constexpr (std::is_same<T, double>::value) {
+        double s, c;
+        sincos(-a, &s, &c);
+        return {c, s};
+    } else {
+        float s, c;
+        sincosf((float)-a, &s, &c);
+        const double cd = c, sd = s;
+        const double k = 1.5 - 0.5 * (cd * cd + sd * sd);  // one Newton step to |f| = 1
+        return {cd * k, sd * k};
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ double decay(double a) {
+    if constexpr (std::is_same<T, double>::value) return exp(-a);
+    else return (double)expf((float)-a);
+}
 
 // ---------------------------------------------------------------- kernel --
 
 constexpr int kMaxPassThreads = 256;
 
-// C = blockDim.x / P lines per CTA (a launch parameter).
+// C = blockDim.x / P lines per tile; CTAs walk tiles with a grid stride.
 template <typename T, int N, int RA, int RB, int P, bool STRIDED>
-__global__ void __launch_bounds__(kMaxPassThreads) k_pass(const PassArgs a) {
+__global__ void __launch_bounds__(kMaxPassThreads, 2) k_pass(const PassArgs a) {
     using L = LineFFT<T, N, RA, RB, P>;
     constexpr int E = L::E;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* smem = reinterpret_cast<T*>(smem_raw);
 
     const int C = blockDim.x / P;
     int c, t;
@@ -198,29 +272,7 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_pass(const PassArgs a) {
         t = threadIdx.x % P;
         c = threadIdx.x / P;
     }
-    T* sre = smem + c * 2 * L::LS;
-    T* sim = sre + L::LS;
-
-    const long line = (long)blockIdx.x * C + c;
-    const long nxy = (long)a.nx * a.ny;
-    long base, stride;
-    int xi = 0, yi = 0, zi = 0;  // line coordinates (the pass axis one is per element)
-    if (a.axis == 0) {
-        yi = (int)(line % a.ny);
-        zi = (int)(line / a.ny);
-        base = line * a.nx;
-        stride = 1;
-    } else if (a.axis == 1) {
-        xi = (int)(line % a.nx);
-        zi = (int)(line / a.nx);
-        base = xi + zi * nxy;
-        stride = a.nx;
-    } else {
-        xi = (int)(line % a.nx);
-        yi = (int)(line / a.nx);
-        base = line;
-        stride = nxy;
-    }
+    cx<T>* sl = reinterpret_cast<cx<T>*>(smem_raw) + c * L::LS;
 
     auto sync = [] {
         if constexpr (STRIDED || P > 32) __syncthreads();
@@ -228,116 +280,170 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_pass(const PassArgs a) {
     };
 
     const cx<T>* __restrict__ tw = reinterpret_cast<const cx<T>*>(a.tw);
-    cx<T> v[E];
-    {
-        const cx<T>* in = reinterpret_cast<const cx<T>*>(a.in) + base;
-#pragma unroll
-        for (int e = 0; e < E; ++e) v[e] = in[(long)L::index(t, e) * stride];
-    }
-
+    const long nxy = (long)a.nx * a.ny;
     KSum acc{0.0, 0.0};
-    const T isn = (T)a.inv_sqrt_n;
 
-    for (int o = 0; o < a.nops; ++o) {
-        switch (a.ops[o]) {
-            case OP_FFT_F: {
-                L::template run<false>(v, t, sre, sim, tw, sync);
+    for (long tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+        const long line = tile * C + c;
+        long base, stride;
+        int xi = 0, yi = 0, zi = 0;  // line coordinates (the pass axis one is per element)
+        if (a.axis == 0) {
+            yi = (int)(line % a.ny);
+            zi = (int)(line / a.ny);
+            base = line * a.nx;
+            stride = 1;
+        } else if (a.axis == 1) {
+            xi = (int)(line % a.nx);
+            zi = (int)(line / a.nx);
+            base = xi + zi * nxy;
+            stride = a.nx;
+        } else {
+            xi = (int)(line % a.nx);
+            yi = (int)(line / a.nx);
+            base = line;
+            stride = nxy;
+        }
+
+        cx<T> v[E];
+        {
+            const cx<T>* in = reinterpret_cast<const cx<T>*>(a.in) + base;
 #pragma unroll
-                for (int e = 0; e < E; ++e) v[e] = cscale(v[e], isn);
-                break;
-            }
-            case OP_FFT_I: {
-                L::template run<true>(v, t, sre, sim, tw, sync);
+            for (int e = 0; e < E; ++e) v[e] = in[(long)L::index(t, e) * stride];
+        }
+
+        for (int o = 0; o < a.nops; ++o) {
+            const int op = a.ops[o];
+            switch (op) {
+                case OP_FFT_F:
+                case OP_FFT_I: {
+                    const bool inv = (op == OP_FFT_I);
+                    if (inv) {
 #pragma unroll
-                for (int e = 0; e < E; ++e) v[e] = cscale(v[e], isn);
-                break;
-            }
-            case OP_SCALE: {
-                const T s = (T)(*a.scale_in);
+                        for (int e = 0; e < E; ++e) v[e].y = -v[e].y;
+                    }
+                    L::forward(v, t, sl, tw, sync);
+                    if (inv) {
 #pragma unroll
-                for (int e = 0; e < E; ++e) v[e] = cscale(v[e], s);
-                break;
-            }
-            case OP_VHALF:
-            case OP_KPHASE: {
-                const void* const* fac = (a.ops[o] == OP_VHALF) ? a.vfac : a.kfac;
-                // factor of the two line coordinates
-                cx<T> lf;
-                if (a.axis == 0) lf = cmul(ldc<T>(fac[1], yi), ldc<T>(fac[2], zi));
-                else if (a.axis == 1) lf = cmul(ldc<T>(fac[0], xi), ldc<T>(fac[2], zi));
-                else lf = cmul(ldc<T>(fac[0], xi), ldc<T>(fac[1], yi));
-                const void* fa = fac[a.axis];
-                const bool nl = (a.ops[o] == OP_VHALF) && a.gpe;
+                        for (int e = 0; e < E; ++e) v[e].y = -v[e].y;
+                    }
+                    break;
+                }
+                case OP_SCALE: {
+                    const T s = (T)(*a.scale_in);
 #pragma unroll
-                for (int e = 0; e < E; ++e) {
-                    cx<T> f = cmul(ldc<T>(fa, L::index(t, e)), lf);
-                    if (nl) {
-                        const T gd = (T)a.nl_coef * (v[e].x * v[e].x + v[e].y * v[e].y);
-                        if (a.gstate == 0) {
-                            f = cscale(f, exp_t(-gd));
-                        } else {
-                            T s, co;
-                            sincos_t(-gd, &s, &co);
-                            f = cmul(f, cx<T>{co, s});
+                    for (int e = 0; e < E; ++e) v[e] = cscale(v[e], s);
+                    break;
+                }
+                case OP_VHALF: {
+                    cx<double> lf;
+                    if (a.axis == 0) lf = cmul(ld2(a.vfac[1], yi), ld2(a.vfac[2], zi));
+                    else if (a.axis == 1) lf = cmul(ld2(a.vfac[0], xi), ld2(a.vfac[2], zi));
+                    else lf = cmul(ld2(a.vfac[0], xi), ld2(a.vfac[1], yi));
+                    const double2* fa = a.vfac[a.axis];
+#pragma unroll
+                    for (int e = 0; e < E; ++e) {
+                        cx<double> f = cmul(ld2(fa, L::index(t, e)), lf);
+                        if (a.gpe) {
+                            const double gd = a.nl_coef * ((double)v[e].x * v[e].x +
+                                                           (double)v[e].y * v[e].y);
+                            if (a.gstate == 0) f = cscale(f, small_decay<T>(gd));
+                            else f = cmul(f, small_phase<T>(gd));
+                        }
+                        v[e] = apply(v[e], f);
+                    }
+                    break;
+                }
+                case OP_KPHASE: {
+                    cx<double> lf;
+                    if (a.axis == 0) lf = cmul(ld2(a.kfac[1], yi), ld2(a.kfac[2], zi));
+                    else if (a.axis == 1) lf = cmul(ld2(a.kfac[0], xi), ld2(a.kfac[2], zi));
+                    else lf = cmul(ld2(a.kfac[0], xi), ld2(a.kfac[1], yi));
+                    lf = cscale(lf, a.kscale_in ? a.kscale * *a.kscale_in : a.kscale);
+                    const double2* fa = a.kfac[a.axis];
+#pragma unroll
+                    for (int e = 0; e < E; ++e) v[e] = apply(v[e], cmul(ld2(fa, L::index(t, e)), lf));
+                    break;
+                }
+                case OP_GAUGE: {
+                    // exp(-A p dt) / exp(-i A p dt) with p = m dp, m the signed
+                    // frequency of index k (m = k - n for k >= n/2): geometric in
+                    // k, so the factor of k = t + P q + r n/RA is
+                    // W^t A^q B^r (times W^-n above n/2) with W = w(dp),
+                    // A = W^P, B = W^(n/RA), formed in FP64.
+                    const int src = a.gauge_src;
+                    const int sidx = (src == 0) ? xi : (src == 1) ? yi : zi;
+                    const double ang1 = a.gauge_coef * a.pos[src][sidx] * a.gauge_dt * a.dmom;
+                    constexpr int QN = E / RA;
+                    if (a.gstate == 0) {
+                        const double wt = exp(-ang1 * t) * a.gscale;
+                        const double wa = exp(-ang1 * P), wb = exp(-ang1 * (N / RA));
+                        const double wn = exp(ang1 * N);
+                        double aq = wt;
+#pragma unroll
+                        for (int q = 0; q < QN; ++q) {
+                            double f = aq;
+#pragma unroll
+                            for (int r = 0; r < RA; ++r) {
+                                const int e = q * RA + r;
+                                const double ff = (t + P * q + r * (N / RA) >= N / 2) ? f * wn : f;
+                                v[e] = apply(v[e], cx<double>{ff, 0.0});
+                                f *= wb;
+                            }
+                            aq *= wa;
+                        }
+                    } else {
+                        cx<double> wt = cscale(unit_phase<double>(ang1 * t), a.gscale);
+                        const cx<double> wa = unit_phase<double>(ang1 * P);
+                        const cx<double> wb = unit_phase<double>(ang1 * (N / RA));
+                        const cx<double> wn = unit_phase<double>(-ang1 * N);
+                        cx<double> aq = wt;
+#pragma unroll
+                        for (int q = 0; q < QN; ++q) {
+                            cx<double> f = aq;
+#pragma unroll
+                            for (int r = 0; r < RA; ++r) {
+                                const int e = q * RA + r;
+                                const cx<double> ff =
+                                    (t + P * q + r * (N / RA) >= N / 2) ? cmul(f, wn) : f;
+                                v[e] = apply(v[e], ff);
+                                f = cmul(f, wb);
+                            }
+                            aq = cmul(aq, wa);
                         }
                     }
-                    v[e] = cmul(f, v[e]);
+                    break;
                 }
-                break;
-            }
-            case OP_GAUGE: {
-                const int src = a.gauge_src;
-                const int sidx = (src == 0) ? xi : (src == 1) ? yi : zi;
-                const double coef = a.gauge_coef * a.pos[src][sidx] * a.gauge_dt;
-                const double* mom = a.mom[a.axis];
+                case OP_NORM: {
 #pragma unroll
-                for (int e = 0; e < E; ++e) {
-                    const T ang = (T)(coef * mom[L::index(t, e)]);
-                    cx<T> f;
-                    if (a.gstate == 0) {
-                        f = cx<T>{exp_t(-ang), (T)0};
-                    } else {
-                        T s, co;
-                        sincos_t(-ang, &s, &co);
-                        f = cx<T>{co, s};
+                    for (int e = 0; e < E; ++e) {
+                        const double re = (double)v[e].x, im = (double)v[e].y;
+                        acc.add(re * re + im * im);
                     }
-                    v[e] = cmul(v[e], f);
+                    break;
                 }
-                break;
-            }
-            case OP_NORM: {
+                case OP_EKIN: {
 #pragma unroll
-                for (int e = 0; e < E; ++e) {
-                    const double re = (double)v[e].x, im = (double)v[e].y;
-                    acc.add(re * re + im * im);
+                    for (int e = 0; e < E; ++e) {
+                        const int k = L::index(t, e);
+                        const double px = a.mom[0][a.axis == 0 ? k : xi];
+                        const double py = a.mom[1][a.axis == 1 ? k : yi];
+                        const double pz = a.mom[2][a.axis == 2 ? k : zi];
+                        const double K = a.kin_coef * (px * px + py * py + pz * pz);
+                        const double re = (double)v[e].x, im = (double)v[e].y;
+                        acc.add(K * (re * re + im * im));
+                    }
+                    break;
                 }
-                break;
+                default:
+                    break;
             }
-            case OP_EKIN: {
-                const double* m0 = a.mom[0];
-                const double* m1 = a.mom[1];
-                const double* m2 = a.mom[2];
-#pragma unroll
-                for (int e = 0; e < E; ++e) {
-                    const int k = L::index(t, e);
-                    const double px = m0[a.axis == 0 ? k : xi];
-                    const double py = m1[a.axis == 1 ? k : yi];
-                    const double pz = m2[a.axis == 2 ? k : zi];
-                    const double K = a.kin_coef * (px * px + py * py + pz * pz);
-                    const double re = (double)v[e].x, im = (double)v[e].y;
-                    acc.add(K * (re * re + im * im));
-                }
-                break;
-            }
-            default:
-                break;
         }
-    }
 
-    if (a.store) {
-        cx<T>* out = reinterpret_cast<cx<T>*>(a.out) + base;
+        if (a.store) {
+            cx<T>* out = reinterpret_cast<cx<T>*>(a.out) + base;
 #pragma unroll
-        for (int e = 0; e < E; ++e) out[(long)L::index(t, e) * stride] = v[e];
+            for (int e = 0; e < E; ++e) out[(long)L::index(t, e) * stride] = v[e];
+        }
     }
 
     if (a.red.kind != RED_NONE) {

@@ -91,7 +91,10 @@ typedef struct gpue_evolve_opts {
     int32_t step_offset;           /* first step index (GPUE starts every evolve() at
                                       0); lets a run continue in slices with the same
                                       time = Dt*i and gauge order i%2 */
-    int32_t reserved[5];
+    int32_t norm_guard;            /* real time only: rescale to the starting norm each
+                                      step (a no-op in exact arithmetic); -1 = on for
+                                      the FP32 form, off for FP64; 0 off; 1 on */
+    int32_t reserved[4];
 } gpue_evolve_opts;
 
 typedef struct gpue_evolve_result {
