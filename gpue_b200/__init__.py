@@ -93,6 +93,8 @@ def lib():
         L.gpue_norm.argtypes = [vp, C.POINTER(C.c_double)]
         L.gpue_ctx_stream.argtypes = [vp, C.POINTER(vp)]
         L.gpue_ctx_wfc_device.argtypes = [vp, C.POINTER(vp), C.POINTER(i32)]
+        L.gpue_norm_noalloc.argtypes = [vp, i32, C.c_int64, C.c_double, vp, vp]
+        L.gpue_norm_noalloc.restype = C.c_int
         for name in ("gpue_default_params", "gpue_ctx_create", "gpue_ctx_destroy",
                      "gpue_set_operators", "gpue_set_wfc", "gpue_get_wfc", "gpue_evolve",
                      "gpue_energy", "gpue_norm", "gpue_ctx_stream", "gpue_ctx_wfc_device"):

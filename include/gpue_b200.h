@@ -150,6 +150,21 @@ gpue_status gpue_ctx_stream(gpue_ctx* ctx, void** stream);
 /* Device pointer of the resident wavefunction and its dtype (GPUE_C128/C64). */
 gpue_status gpue_ctx_wfc_device(gpue_ctx* ctx, void** psi, int32_t* dtype);
 
+/* No counterpart in GPUE: sum |psi|^2 * dV of a wavefunction the caller owns
+ * on the current device, written to *out (device memory the caller owns),
+ * for callers that must not trigger any device allocation, such as a server
+ * that reserved its whole memory budget up front.  The library allocates
+ * nothing here: the reduction scratch is a fixed 1 MiB device array that
+ * every GPU loading the library holds until exit, which caps npoints at
+ * 2^28 (larger sizes return GPUE_ERR_INVALID_ARG with a message on stderr).
+ * Asynchronous on `stream` (a cudaStream_t, may be NULL).  The first call on
+ * a device looks up the array's device address; make that first call before
+ * any stream capture.  All calls share the array, so calls whose kernels can
+ * overlap on the GPU race; order them on one stream.  dtype is GPUE_C128 or
+ * GPUE_C64. */
+gpue_status gpue_norm_noalloc(const void* psi, int32_t dtype, int64_t npoints, double dV,
+                              double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
