@@ -118,3 +118,30 @@ def test_fp32_roundtrip_and_dtypes(G):
         assert np.array_equal(b64, psi0.astype(np.complex64))
         b128 = s.get_wfc(np.complex128)
         assert np.array_equal(b128, psi0.astype(np.complex64).astype(np.complex128))
+
+
+def test_fp32_ground_state_energy_gate(G):
+    """Converged ground state: the fused FP32 form is within 1e-6 relative of
+    the plain FP64 energy on its own (measured ~1e-7), and FP64 polishing
+    steps that replace the last 100 steps bring it to ~5e-9."""
+    c = dict(cases.DEFAULTS, dim=2, n=128, box=8.0, g=100.0, gdt=1e-3, seed=41, init="gauss")
+    from helpers import product_params
+    S = 40000
+    psi0 = cases.initial_psi(c)
+    with G.Solver(product_params(c, G.PREC_FP64)) as s:
+        s.set_wfc(psi0)
+        s.evolve(S, 0)
+        E64 = s.energy()
+    with G.Solver(product_params(c, G.PREC_FP32)) as s:
+        s.set_wfc(psi0)
+        s.evolve(S, 0)
+        E32 = s.energy()
+    with G.Solver(product_params(c, G.PREC_FP32)) as s:
+        s.set_wfc(psi0)
+        r = s.evolve(S - 100, 0, polish_steps=100)
+        E32p = s.energy()
+        psi = s.get_wfc()
+    assert r["steps_done"] == S
+    assert abs(E32 - E64) <= 1e-6 * abs(E64)
+    assert abs(E32p - E64) <= 1e-7 * abs(E64)
+    assert psi.dtype == np.complex128
