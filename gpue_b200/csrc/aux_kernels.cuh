@@ -28,6 +28,8 @@ struct EnergyArgs {
     double dx, dy, dz;
     double hbar;
     RedArgs red;
+    const double* vtab;     // full-field V (parameter-file form), else separable
+    const double* atab[3];  // full-field A (parameter-file form), else rotation
 };
 
 template <typename T>
@@ -45,7 +47,7 @@ __global__ void __launch_bounds__(256) k_energy_real(const EnergyArgs a) {
         const cx<T> pv = psi[g];
         const double px = s * (double)pv.x, py = s * (double)pv.y;
         const double r = px * px + py * py;
-        const double V = a.vreal[0][xi] + a.vreal[1][yi] + a.vreal[2][zi];
+        const double V = a.vtab ? a.vtab[g] : a.vreal[0][xi] + a.vreal[1][yi] + a.vreal[2][zi];
         double e = a.gpe ? r * (V + 0.5 * a.gN * r) : r * V;
         if (a.lterm) {
             auto dfwd = [&](long stride, double d, double& ox, double& oy) {
@@ -61,10 +63,16 @@ __global__ void __launch_bounds__(256) k_energy_real(const EnergyArgs a) {
             double dxr, dxi, dyr, dyi;
             dfwd(1, a.dx, dxr, dxi);
             dfwd(a.nx, a.dy, dyr, dyi);
-            const double Ax = a.ax_coef * a.pos[1][yi];
-            const double Ay = a.ay_coef * a.pos[0][xi];
+            const double Ax = a.atab[0] ? a.atab[0][g] : a.ax_coef * a.pos[1][yi];
+            const double Ay = a.atab[1] ? a.atab[1][g] : a.ay_coef * a.pos[0][xi];
             double lr = dxr * Ax + dyr * Ay;
             double li = dxi * Ax + dyi * Ay;
+            if (a.dim == 3 && a.atab[2]) {
+                double dzr, dzi;
+                dfwd(nxy, a.dz, dzr, dzi);
+                lr += dzr * a.atab[2][g];
+                li += dzi * a.atab[2][g];
+            }
             // i*hbar*l, then Re[conj(p) * (i hbar l)]
             const double ir = -a.hbar * li, ii = a.hbar * lr;
             e += px * ir + py * ii;

@@ -32,7 +32,10 @@
 #include <string>
 #include <vector>
 
+#include <cctype>
+
 #include "../../include/gpue_b200.h"
+#include "ast.h"
 #include "aux_kernels.cuh"
 #include "registry.h"
 
@@ -108,6 +111,16 @@ struct gpue_ctx {
     std::string err;
     long launches = 0;         // kernels enqueued in the current evolve call
     double last_energy = 0.0;  // energy of the latest check (GPUE's "energy" key)
+    // parameter-file fields (gpue_load_param_text)
+    bool ext = false;          // passes use the table / expression forms
+    double* vtab = nullptr;    // static V(g) and A_a(g) (FP64, N each)
+    double* atab[3] = {};
+    bool use_atab = false;     // gauge from the A tables instead of the rotation preset
+    bool atab_nonzero[3] = {};
+    AstInstr* progs = nullptr; // device copy of the time-dependent programs
+    int prog_off[5] = {-1, -1, -1, -1, -1};  // V, k, Ax, Ay, Az
+    int prog_len[5] = {};
+    bool time_dep = false;     // some factor is evaluated per step
 };
 
 namespace {
@@ -180,6 +193,15 @@ void build_axis(Axis& a, int n, double xmax, bool active) {
 
 bool gauge_active(const gpue_ctx* c) {
     return c->p.corotating && c->p.gauge == GPUE_GAUGE_ROTATION && c->p.omega != 0.0;
+}
+
+// Does the gauge pass along `axis` change the state?  Preset rotation: x and
+// y when omega != 0; parameter-file fields: a time-dependent expression, or a
+// static table that is not identically zero.
+bool axis_gauge_active(const gpue_ctx* c, int axis) {
+    if (c->prog_off[2 + axis] >= 0) return true;
+    if (c->use_atab) return c->atab_nonzero[axis];
+    return axis < 2 && gauge_active(c);
 }
 
 // A = (ax_coef * y, ay_coef * x, 0) for the rotation gauge (krotation_Ax/Ay,
@@ -346,6 +368,7 @@ struct LPass {
     double gauge_dt = 0;       // for OP_GAUGE
     int scale_slot = kScale;   // OP_SCALE factor
     int kscale_slot = -1;      // extra factor folded into OP_KPHASE (norm guard)
+    double time = 0;           // Dt * step, for time-dependent expressions
 };
 
 gpue_status launch_pass(gpue_ctx* c, int prec, const LPass& lp, int gstate) {
@@ -395,7 +418,26 @@ gpue_status launch_pass(gpue_ctx* c, int prec, const LPass& lp, int gstate) {
     a.red.target = c->scal + lp.red_target;
     a.scale_in = c->scal + lp.scale_slot;
     a.kscale_in = lp.kscale_slot >= 0 ? c->scal + lp.kscale_slot : nullptr;
-    void (*fn)(PassArgs) = lp.axis == 0 ? lc.k->row : lc.k->col;
+    a.hbar = p.hbar;
+    a.step_dt = Dt;
+    a.time = lp.time;
+    // evolve() passes dx, and dy/dz only where the axis exists (1 otherwise)
+    a.grid_d[0] = c->ax[0].dx;
+    a.grid_d[1] = c->dim > 1 ? c->ax[1].dx : 1.0;
+    a.grid_d[2] = c->dim > 2 ? c->ax[2].dx : 1.0;
+    if (c->ext) {
+        a.vtab = c->vtab;
+        for (int i = 0; i < 3; ++i) a.atab[i] = c->use_atab ? c->atab[i] : nullptr;
+        auto prog = [&](int k, const AstInstr*& pp, int& n) {
+            pp = c->prog_off[k] >= 0 ? c->progs + c->prog_off[k] : nullptr;
+            n = c->prog_len[k];
+        };
+        prog(0, a.prog_v, a.nprog_v);
+        prog(1, a.prog_k, a.nprog_k);
+        for (int i = 0; i < 3; ++i) prog(2 + i, a.prog_a[i], a.nprog_a[i]);
+    }
+    void (*fn)(PassArgs) = lp.axis == 0 ? (c->ext ? lc.k->row_ext : lc.k->row)
+                                        : (c->ext ? lc.k->col_ext : lc.k->col);
     fn<<<lc.blocks, lc.threads, lc.smem, c->stream>>>(a);
     c->launches++;
     CK(cudaGetLastError());
@@ -407,21 +449,30 @@ gpue_status launch_pass(gpue_ctx* c, int prec, const LPass& lp, int gstate) {
 void step_passes(gpue_ctx* c, int i, int gstate, bool scale_first, double rexp, bool guard,
                  std::vector<LPass>& out) {
     const bool imag = gstate == 0;
-    const bool g = gauge_active(c);
     const double gdt = imag ? c->p.gdt * rexp : c->p.dt;
+    const double tnow = (imag ? c->p.gdt : c->p.dt) * i;
     auto P = [&](int axis, std::vector<int> ops) {
         LPass lp;
         lp.axis = axis;
         lp.ops = ops;
         lp.gauge_dt = gdt;
+        lp.time = tnow;
         return lp;
     };
+    // gauge axes in GPUE's order for this step (x,y,z when i is odd, z,y,x
+    // otherwise), leaving out axes whose factor is identically 1
+    std::vector<int> gaxes;
+    if (c->p.corotating) {
+        const int order1[3] = {0, 1, 2}, order0[3] = {2, 1, 0};
+        const int* ord = (i % 2) ? order1 : order0;
+        for (int k = 0; k < 3; ++k)
+            if (ord[k] < c->dim && axis_gauge_active(c, ord[k])) gaxes.push_back(ord[k]);
+    }
     std::vector<LPass> s;
     std::vector<int> first;
     if (scale_first) first.push_back(OP_SCALE);
     first.push_back(OP_VHALF);
     first.push_back(OP_FFT_F);
-    const bool flip = (i % 2) != 0;
     const int kaxis = c->dim == 3 ? 2 : 1;
     s.push_back(P(0, first));
     if (c->dim == 3) s.push_back(P(1, {OP_FFT_F}));
@@ -429,16 +480,14 @@ void step_passes(gpue_ctx* c, int i, int gstate, bool scale_first, double rexp, 
     if (guard) kp.kscale_slot = kGuard;
     s.push_back(kp);
     if (c->dim == 3) s.push_back(P(1, {OP_FFT_I}));
-    if (g && flip) {
+    size_t g0 = 0;
+    if (!gaxes.empty() && gaxes[0] == 0) {
         s.push_back(P(0, {OP_FFT_I, OP_VHALF, OP_FFT_F, OP_GAUGE, OP_FFT_I}));
-        s.push_back(P(1, {OP_FFT_F, OP_GAUGE, OP_FFT_I}));
-    } else if (g) {
-        s.push_back(P(0, {OP_FFT_I, OP_VHALF}));
-        s.push_back(P(1, {OP_FFT_F, OP_GAUGE, OP_FFT_I}));
-        s.push_back(P(0, {OP_FFT_F, OP_GAUGE, OP_FFT_I}));
+        g0 = 1;
     } else {
         s.push_back(P(0, {OP_FFT_I, OP_VHALF}));
     }
+    for (size_t k = g0; k < gaxes.size(); ++k) s.push_back(P(gaxes[k], {OP_FFT_F, OP_GAUGE, OP_FFT_I}));
     if (imag || guard) {
         LPass& last = s.back();
         last.ops.push_back(OP_NORM);
@@ -534,6 +583,13 @@ gpue_status launch_energy(gpue_ctx* c, int prec, int gstate, bool scale_pending)
     e.lterm = (c->p.corotating && c->dim > 1 && (axc != 0.0 || ayc != 0.0)) ? 1 : 0;
     e.ax_coef = axc;
     e.ay_coef = ayc;
+    if (c->ext) {
+        e.vtab = c->vtab;
+        if (c->use_atab) {
+            for (int i = 0; i < 3; ++i) e.atab[i] = c->atab[i];
+            e.lterm = (c->p.corotating && c->dim > 1) ? 1 : 0;
+        }
+    }
     e.dx = c->ax[0].dx;
     e.dy = c->ax[1].dx;
     e.dz = c->ax[2].dx;
@@ -612,7 +668,7 @@ gpue_status enqueue_steps(gpue_ctx* c, int prec, int i0, int i1, int gstate, boo
     for (int i = i0; i < i1; ++i)
         step_passes(c, i, gstate, i == i0 ? scale_first : gstate == 0,
                     rexp.empty() ? 1.0 : rexp[i], guard, v);
-    fuse(v);
+    if (!c->time_dep) fuse(v);  // fused passes would mix two steps' times
     for (auto& lp : v) {
         gpue_status st = launch_pass(c, prec, lp, gstate);
         if (st) return st;
@@ -626,7 +682,8 @@ gpue_status enqueue_steps(gpue_ctx* c, int prec, int i0, int i1, int gstate, boo
 
 gpue_status run_segment(gpue_ctx* c, int prec, int i0, int i1, int gstate, bool scale_first,
                         const std::vector<double>& rexp, bool energy_after, bool guard) {
-    if (!rexp.empty())
+    // per-step arguments (ramp exponent, expression time) are not cached
+    if (!rexp.empty() || c->time_dep)
         return enqueue_steps(c, prec, i0, i1, gstate, scale_first, rexp, energy_after, guard);
     GraphKey key{prec, gstate, i0 % 2, i1 - i0, scale_first ? 1 : 0, energy_after ? 1 : 0,
                  guard ? 1 : 0};
@@ -675,7 +732,8 @@ gpue_status step_loop(gpue_ctx* c, int prec, int off, int nsteps, int gstate,
     std::vector<double> rexp;
     // ramp (src/evolution.cu:409-427): GPUE raises the gauge tables to
     // omega_0 every step, so the exponent at step i is cumulative
-    if (c->p.ramp && gstate == 0 && gauge_active(c)) {
+    if (c->p.ramp && gstate == 0 && c->p.corotating &&
+        (axis_gauge_active(c, 0) || axis_gauge_active(c, 1) || axis_gauge_active(c, 2))) {
         rexp.resize(last);
         double r = 1.0;
         for (int i = 0; i < last; ++i) {
@@ -852,6 +910,10 @@ gpue_status gpue_ctx_destroy(gpue_ctx* c) {
         if (t.buf) cudaFree(t.buf);
     cudaFree(c->psi);
     if (c->psi64) cudaFree(c->psi64);
+    if (c->vtab) cudaFree(c->vtab);
+    for (auto t : c->atab)
+        if (t) cudaFree(t);
+    if (c->progs) cudaFree(c->progs);
     cudaFree(c->scratch);
     cudaFree(c->scal);
     cudaFree(c->partials);
@@ -952,6 +1014,134 @@ gpue_status gpue_ctx_stream(gpue_ctx* c, void** s) {
     return GPUE_OK;
 }
 
+// The Grid doubles an expression may name (parseArgs and init() store them).
+static std::map<std::string, double> grid_doubles(const gpue_ctx* c, const char* const* names,
+                                                  const double* values, int32_t n) {
+    const gpue_params& p = c->p;
+    std::map<std::string, double> m = {
+        {"omega", p.omega},       {"gammaY", p.gammaY},       {"gdt", p.gdt},
+        {"dt", p.dt},             {"omegaX", p.omegaX},       {"omegaY", p.omegaY},
+        {"omegaZ", p.omegaZ},     {"interaction", p.interaction},
+        {"x0_shift", p.x0_shift}, {"y0_shift", p.y0_shift},   {"z0_shift", p.z0_shift},
+        {"mass", p.mass},         {"gDenConst", p.gDenConst}, {"xMax", p.xMax},
+        {"yMax", p.yMax},         {"zMax", p.zMax},           {"dx", c->ax[0].dx},
+        {"dy", c->ax[1].dx},      {"dz", c->dim == 3 ? c->ax[2].dx : 1.0},
+        {"fudge", 0.0}};
+    for (int a = 0; a < 3; ++a) {
+        const char* nm[3][2] = {{"dpx", "pxMax"}, {"dpy", "pyMax"}, {"dpz", "pzMax"}};
+        const double xm = a == 0 ? p.xMax : a == 1 ? p.yMax : p.zMax;
+        const int na = a == 0 ? p.xDim : a == 1 ? p.yDim : p.zDim;
+        if (xm > 0) {
+            m[nm[a][0]] = kPI / xm;
+            m[nm[a][1]] = (kPI / xm) * (na >> 1);
+        }
+    }
+    for (int i = 0; i < n; ++i)
+        if (names && names[i] && values) m[names[i]] = values[i];
+    return m;
+}
+
+gpue_status gpue_load_param_text(gpue_ctx* c, const char* text, int32_t time_mode,
+                                 const char* const* names, const double* values,
+                                 int32_t nvalues) {
+    if (!c || !text || (time_mode != 0 && time_mode != 1) || nvalues < 0)
+        return GPUE_ERR_INVALID_ARG;
+    CK(cudaSetDevice(c->device));
+    std::map<std::string, AstExpr> ex;
+    std::vector<std::string> order;
+    std::string err;
+    if (!ast_parse_file(text, grid_doubles(c, names, values, nvalues), ex, order, err))
+        return fail(c, GPUE_ERR_AST, "%s", err.c_str());
+    const gpue_params& p = c->p;
+    const int nx = c->ax[0].n, ny = c->ax[1].n, nz = c->ax[2].n;
+    const double dx = c->ax[0].dx, dy = c->ax[1].dx, dz = c->dim == 3 ? c->ax[2].dx : 1.0;
+    const double zmax = c->dim == 3 ? p.zMax : 0.0;
+    auto has = [&](const char* k) { return ex.count(k) > 0; };
+    // static fields at t = 0 (find_field, src/dynamic.cu:605-616; generate_gauge
+    // and generate_fields, src/operators.cu:472-618, 808-830)
+    std::vector<double> V(c->N), A[3];
+    for (auto& v : A) v.assign(c->N, 0.0);
+    double axc, ayc;
+    gauge_coefs(c, axc, ayc);
+    const bool any_a = has("Ax") || has("Ay") || has("Az");
+    const char* an[3] = {"Ax", "Ay", "Az"};
+    for (long g = 0; g < c->N; ++g) {
+        const int i = (int)(g % nx), j = (int)((g / nx) % ny), k = (int)(g / ((long)nx * ny));
+        const double fx = dx * i - p.xMax, fy = dy * j - p.yMax, fz = dz * k - zmax;
+        for (int a = 0; a < 3; ++a) {
+            if (has(an[a])) A[a][g] = ast_eval_host(ex[an[a]], fx, fy, fz, 0.0);
+            else if (a == 0) A[a][g] = -c->ax[1].x[j] * p.omega * p.omegaX * (axc != 0.0);
+            else if (a == 1) A[a][g] = c->ax[0].x[i] * p.omega * p.omegaY * (ayc != 0.0);
+        }
+        if (has("V")) {
+            V[g] = ast_eval_host(ex["V"], fx, fy, fz, 0.0);
+        } else {
+            const double vx = p.omegaX * (c->ax[0].x[i] + p.x0_shift);
+            const double vy = p.gammaY * p.omegaY * (c->ax[1].x[j] + p.y0_shift);
+            const double vz = (c->dim == 3 ? p.omegaZ : 0.0) *
+                              (c->ax[2].x[k] + (c->dim == 3 ? p.z0_shift : 0.0));
+            V[g] = 0.5 * p.mass * ((vx * vx + vy * vy + vz * vz) +
+                                   (A[0][g] * A[0][g] + A[1][g] * A[1][g] + A[2][g] * A[2][g]));
+        }
+    }
+    if (!c->vtab) {
+        CK(cudaMalloc(&c->vtab, c->N * sizeof(double)));
+        for (auto& t : c->atab) CK(cudaMalloc(&t, c->N * sizeof(double)));
+    }
+    CK(cudaMemcpy(c->vtab, V.data(), c->N * sizeof(double), cudaMemcpyHostToDevice));
+    for (int a = 0; a < 3; ++a) {
+        CK(cudaMemcpy(c->atab[a], A[a].data(), c->N * sizeof(double), cudaMemcpyHostToDevice));
+        bool nz_any = false;
+        for (double v : A[a]) nz_any |= (v != 0.0);
+        c->atab_nonzero[a] = nz_any;
+    }
+    c->use_atab = any_a;
+    // time-dependent expressions: evolve()'s *_time branches
+    std::vector<AstInstr> progs;
+    const char* pn[5] = {"V", "k", "Ax", "Ay", "Az"};
+    c->time_dep = false;
+    for (int k = 0; k < 5; ++k) {
+        c->prog_off[k] = -1;
+        c->prog_len[k] = 0;
+        if (time_mode == 1 && has(pn[k]) && ex[pn[k]].time_dependent) {
+            c->prog_off[k] = (int)progs.size();
+            c->prog_len[k] = (int)ex[pn[k]].program.size();
+            for (auto& in : ex[pn[k]].program) progs.push_back(in);
+            c->time_dep = true;
+        }
+    }
+    if (c->progs) {
+        cudaFree(c->progs);
+        c->progs = nullptr;
+    }
+    if (!progs.empty()) {
+        CK(cudaMalloc(&c->progs, progs.size() * sizeof(AstInstr)));
+        CK(cudaMemcpy(c->progs, progs.data(), progs.size() * sizeof(AstInstr),
+                      cudaMemcpyHostToDevice));
+    }
+    c->ext = true;
+    destroy_graphs(c);
+    return GPUE_OK;
+}
+
+gpue_status gpue_ast_parse(const char* expr, const char* const* names, const double* values,
+                           int32_t nvalues, void* nodes_out, int32_t cap, int32_t* count) {
+    if (!expr || !count || cap < 0 || nvalues < 0) return GPUE_ERR_INVALID_ARG;
+    std::map<std::string, double> m;
+    for (int i = 0; i < nvalues; ++i)
+        if (names && names[i] && values) m[names[i]] = values[i];
+    std::string s;
+    for (const char* q = expr; *q; ++q)
+        if (!std::isspace((unsigned char)*q)) s.push_back(*q);
+    AstExpr e;
+    std::string err;
+    if (!ast_parse(s, m, e, err)) return GPUE_ERR_AST;
+    *count = (int32_t)e.nodes.size();
+    if (nodes_out && cap >= *count) std::memcpy(nodes_out, e.nodes.data(), e.nodes.size() * sizeof(AstNode));
+    else if (nodes_out) return GPUE_ERR_INVALID_ARG;
+    return GPUE_OK;
+}
+
 gpue_status gpue_ctx_wfc_device(gpue_ctx* c, void** psi, int32_t* dtype) {
     if (!c || !psi || !dtype) return GPUE_ERR_INVALID_ARG;
     *psi = c->psi;
@@ -1049,10 +1239,14 @@ gpue_status gpue_evolve(gpue_ctx* c, int32_t nsteps, int32_t gstate,
 namespace gpue {
 
 const PassKernel* find_pass_kernel(int prec, int n) {
-    int cnt = 0;
-    const PassKernel* t = prec == PREC_F32 ? pass_table_f32(&cnt) : pass_table_f64(&cnt);
-    for (int i = 0; i < cnt; ++i)
-        if (t[i].n == n) return &t[i];
+    for (int part = 0; part < 2; ++part) {
+        int cnt = 0;
+        const PassKernel* t =
+            prec == PREC_F32 ? (part ? pass_table_f32_b(&cnt) : pass_table_f32_a(&cnt))
+                             : (part ? pass_table_f64_b(&cnt) : pass_table_f64_a(&cnt));
+        for (int i = 0; i < cnt; ++i)
+            if (t[i].n == n) return &t[i];
+    }
     return nullptr;
 }
 

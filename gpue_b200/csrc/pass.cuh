@@ -34,6 +34,7 @@
 
 #include <type_traits>
 
+#include "ast_eval.cuh"
 #include "fft_core.cuh"
 
 namespace gpue {
@@ -91,6 +92,20 @@ struct PassArgs {
     RedArgs red;
     const double* scale_in;   // OP_SCALE factor
     const double* kscale_in;  // optional extra OP_KPHASE factor (real-time norm guard)
+    // Extended forms (kernels built with EXT only): full-field tables of real
+    // V and A (GPUE's static param-file fields, find_field at t = 0) and
+    // time-dependent expressions evaluated per point and step at (i dx, j dy,
+    // k dz, t) as evolve()'s AST kernels do.
+    const double* vtab;      // V(g), replaces the separable V
+    const double* atab[3];   // A_axis(g), replaces the rotation gauge
+    const AstInstr* prog_v;  // time-dependent V
+    const AstInstr* prog_k;  // time-dependent K
+    const AstInstr* prog_a[3];
+    int nprog_v, nprog_k, nprog_a[3];
+    double time;             // Dt * step
+    double step_dt;          // Dt
+    double grid_d[3];        // dx, dy, dz as evolve() passes them (1 for absent axes)
+    double hbar;
 };
 
 // ------------------------------------------------------- FP64 reductions --
@@ -257,7 +272,16 @@ __device__ __forceinline__ double decay(double a) {
 constexpr int kMaxPassThreads = 256;
 
 // C = blockDim.x / P lines per tile; CTAs walk tiles with a grid stride.
-template <typename T, int N, int RA, int RB, int P, bool STRIDED>
+// make_complex (src/kernels.cu:165-187): 1 -> exp(-v), 2 -> exp(-i v)
+__device__ __forceinline__ cx<double> make_complex_ev(double v, int type) {
+    if (type == 1) return {exp(-v), 0.0};
+    double s, c;
+    sincos(-v, &s, &c);
+    return {c, s};
+}
+
+// EXT: also the table and expression forms of the factor ops.
+template <typename T, int N, int RA, int RB, int P, bool STRIDED, bool EXT>
 __global__ void __launch_bounds__(kMaxPassThreads, 2) k_pass(const PassArgs a) {
     using L = LineFFT<T, N, RA, RB, P>;
     constexpr int E = L::E;
@@ -335,6 +359,41 @@ __global__ void __launch_bounds__(kMaxPassThreads, 2) k_pass(const PassArgs a) {
                     break;
                 }
                 case OP_VHALF: {
+                    if constexpr (EXT) {
+                        if (a.prog_v || a.vtab) {
+                            // cMultDensity_ast (src/kernels.cu:391-422): V(x,t) with no
+                            // dt factor; linear: ast_op_mult with the full Dt.  Static
+                            // tables: the aux_fields factors of V(g).
+                            const double* d = a.grid_d;
+#pragma unroll
+                            for (int e = 0; e < E; ++e) {
+                                const int k = L::index(t, e);
+                                cx<double> f;
+                                if (a.prog_v) {
+                                    const double px = (a.axis == 0 ? k : xi) * d[0];
+                                    const double py = (a.axis == 1 ? k : yi) * d[1];
+                                    const double pz = (a.axis == 2 ? k : zi) * d[2];
+                                    const double val =
+                                        ast_eval(a.prog_v, a.nprog_v, px, py, pz, a.time);
+                                    f = make_complex_ev(a.gpe ? val : val * a.step_dt,
+                                                        a.gstate + 1);
+                                } else {
+                                    const double V = a.vtab[base + (long)k * stride];
+                                    const double ang = V * (a.step_dt / (2.0 * a.hbar));
+                                    f = a.gstate == 0 ? cx<double>{small_decay<T>(ang), 0.0}
+                                                      : small_phase<T>(ang);
+                                }
+                                if (a.gpe) {
+                                    const double gd = a.nl_coef * ((double)v[e].x * v[e].x +
+                                                                   (double)v[e].y * v[e].y);
+                                    if (a.gstate == 0) f = cscale(f, small_decay<T>(gd));
+                                    else f = cmul(f, small_phase<T>(gd));
+                                }
+                                v[e] = apply(v[e], f);
+                            }
+                            break;
+                        }
+                    }
                     cx<double> lf;
                     if (a.axis == 0) lf = cmul(ld2(a.vfac[1], yi), ld2(a.vfac[2], zi));
                     else if (a.axis == 1) lf = cmul(ld2(a.vfac[0], xi), ld2(a.vfac[2], zi));
@@ -354,6 +413,26 @@ __global__ void __launch_bounds__(kMaxPassThreads, 2) k_pass(const PassArgs a) {
                     break;
                 }
                 case OP_KPHASE: {
+                    if constexpr (EXT) {
+                        if (a.prog_k) {
+                            // ast_op_mult with the "k" expression at the position
+                            // coordinates of the indices (src/evolution.cu:764-768)
+                            const double* d = a.grid_d;
+                            const double ks = a.kscale_in ? a.kscale * *a.kscale_in : a.kscale;
+#pragma unroll
+                            for (int e = 0; e < E; ++e) {
+                                const int k = L::index(t, e);
+                                const double px = (a.axis == 0 ? k : xi) * d[0];
+                                const double py = (a.axis == 1 ? k : yi) * d[1];
+                                const double pz = (a.axis == 2 ? k : zi) * d[2];
+                                const double val =
+                                    ast_eval(a.prog_k, a.nprog_k, px, py, pz, a.time);
+                                v[e] = apply(v[e], cscale(make_complex_ev(val * a.step_dt,
+                                                                          a.gstate + 1), ks));
+                            }
+                            break;
+                        }
+                    }
                     cx<double> lf;
                     if (a.axis == 0) lf = cmul(ld2(a.kfac[1], yi), ld2(a.kfac[2], zi));
                     else if (a.axis == 1) lf = cmul(ld2(a.kfac[0], xi), ld2(a.kfac[2], zi));
@@ -365,6 +444,33 @@ __global__ void __launch_bounds__(kMaxPassThreads, 2) k_pass(const PassArgs a) {
                     break;
                 }
                 case OP_GAUGE: {
+                    if constexpr (EXT) {
+                        if (a.prog_a[a.axis] || a.atab[a.axis]) {
+                            // ast_cmult multiplies by the raw A(x,t) (src/kernels.cu:
+                            // 632-645); tables give exp(-A(g) p_k dt) per point
+                            const double* d = a.grid_d;
+                            const AstInstr* pr = a.prog_a[a.axis];
+                            const double* mom = a.mom[a.axis];
+#pragma unroll
+                            for (int e = 0; e < E; ++e) {
+                                const int k = L::index(t, e);
+                                cx<double> f;
+                                if (pr) {
+                                    const double px = (a.axis == 0 ? k : xi) * d[0];
+                                    const double py = (a.axis == 1 ? k : yi) * d[1];
+                                    const double pz = (a.axis == 2 ? k : zi) * d[2];
+                                    f = {ast_eval(pr, a.nprog_a[a.axis], px, py, pz, a.time), 0.0};
+                                } else {
+                                    const double ang =
+                                        a.atab[a.axis][base + (long)k * stride] * mom[k] * a.gauge_dt;
+                                    f = a.gstate == 0 ? cx<double>{small_decay<T>(ang), 0.0}
+                                                      : small_phase<T>(ang);
+                                }
+                                v[e] = apply(v[e], cscale(f, a.gscale));
+                            }
+                            break;
+                        }
+                    }
                     // exp(-A p dt) / exp(-i A p dt) with p = m dp, m the signed
                     // frequency of index k (m = k - n for k >= n/2): geometric in
                     // k, so the factor of k = t + P q + r n/RA is

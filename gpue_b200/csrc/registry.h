@@ -16,6 +16,8 @@ struct PassKernel {
     int elem;     // bytes per complex element
     void (*row)(PassArgs);
     void (*col)(PassArgs);
+    void (*row_ext)(PassArgs);  // with table / expression factor forms
+    void (*col_ext)(PassArgs);
 };
 
 // nullptr when the length has no compiled plan
@@ -23,7 +25,16 @@ const PassKernel* find_pass_kernel(int prec, int n);
 // supported line lengths, ascending; returns the count
 int supported_lengths(int prec, const int** out);
 
-const PassKernel* pass_table_f32(int* count);
-const PassKernel* pass_table_f64(int* count);
+// The tables are split by length over translation units so they compile in
+// parallel: _a holds lengths <= 192, _b lengths >= 256.
+const PassKernel* pass_table_f32_a(int* count);
+const PassKernel* pass_table_f32_b(int* count);
+const PassKernel* pass_table_f64_a(int* count);
+const PassKernel* pass_table_f64_b(int* count);
+
+#define GPUE_PLAN(T, N, RA, RB, P)                                                        \
+    PassKernel{N, RA, RB, P, LineFFT<T, N, RA, RB, P>::LS, (int)sizeof(cx<T>),            \
+               &k_pass<T, N, RA, RB, P, false, false>, &k_pass<T, N, RA, RB, P, true, false>, \
+               &k_pass<T, N, RA, RB, P, false, true>, &k_pass<T, N, RA, RB, P, true, true>}
 
 }  // namespace gpue

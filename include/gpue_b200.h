@@ -147,6 +147,27 @@ gpue_status gpue_norm(gpue_ctx* ctx, double* norm);
 /* The context's cudaStream_t (as void*) for callers that time or order work. */
 gpue_status gpue_ctx_stream(gpue_ctx* ctx, void** stream);
 
+/* Parameter-file fields (GPUE's -I file: parse_param_file, src/dynamic.cu:187-222,
+ * used by init() and generate_fields, src/init.cu:199-201,
+ * src/operators.cu:472-618,808-830).  `text` holds "name = expr" lines in GPUE's
+ * grammar; V, Ax, Ay, Az are evaluated once at t = 0 on the grid
+ * (x = dx*i - xMax, ...) and replace the harmonic trap / preset gauge, with V
+ * getting +0.5*mass*(Ax*Ax+Ay*Ay+Az*Az) unless it is the last entry, as GPUE
+ * does.  time_mode 0 keeps GPUE's main() behaviour (static fields only);
+ * time_mode 1 also evaluates every time-dependent entry (V, k, Ax, Ay, Az) per
+ * point and step as evolve()'s AST kernels do (src/kernels.cu:391-422,632-665).
+ * names/values add Grid doubles the expressions may use. */
+gpue_status gpue_load_param_text(gpue_ctx* ctx, const char* text, int32_t time_mode,
+                                 const char* const* names, const double* values,
+                                 int32_t nvalues);
+
+/* parse_eqn + tree_to_array (src/dynamic.cu:227-507) of one expression into
+ * GPUE's flat EqnNode_gpu layout {double val; int32 is_dynamic; int32 var;
+ * int32 left; int32 right; int32 op_num} (32 bytes each); no device work.
+ * *count receives the node count; nodes_out may be NULL to query it. */
+gpue_status gpue_ast_parse(const char* expr, const char* const* names, const double* values,
+                           int32_t nvalues, void* nodes_out, int32_t cap, int32_t* count);
+
 /* Device pointer of the resident wavefunction and its dtype (GPUE_C128/C64). */
 gpue_status gpue_ctx_wfc_device(gpue_ctx* ctx, void** psi, int32_t* dtype);
 

@@ -1,0 +1,130 @@
+"""Parameter-file fields through the C ABI against the oracle.
+
+Static fields (GPUE's main() path: find_field at t = 0, src/dynamic.cu:605-616)
+and the time-dependent branches of evolve() (cMultDensity_ast, ast_op_mult,
+ast_cmult; src/kernels.cu:391-422, 632-665), which GPUE's main() cannot reach
+because init() resets the *_time flags; time_mode = 1 turns them on.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import ast_oracle
+import cases
+import oracle
+from helpers import l2, oracle_problem, product_params
+
+pytestmark = pytest.mark.gpu
+
+
+def doubles_for(c):
+    return {"omega": c["omega"], "omegaX": c["wx"], "omegaY": c["wy"], "omegaZ": c["wz"],
+            "mass": 1.0, "xMax": c["box"], "yMax": c["box"], "gammaY": c["gamma"]}
+
+
+def find_field(rows, c):
+    """Field on GPUE's find_field positions (dx*i - xMax, dy*j - yMax, 0)."""
+    n, box = c["n"], c["box"]
+    dx = box / (n >> 1)
+    arr = oracle.nodes_array(rows)
+    out = np.empty(n * n)
+    f = oracle.lib().orc_ast_eval
+    for j in range(n):
+        for i in range(n):
+            out[i + n * j] = f(arr, dx * i - box, dx * j - box, 0.0, 0.0)
+    return out
+
+
+def run(c, prec, text=None, time_mode=0, steps=None):
+    import gpue_b200 as G
+    steps = steps or (c["gsteps"] or c["esteps"])
+    gs = 0 if c["gsteps"] else 1
+    with G.Solver(product_params(c, prec)) as s:
+        if text is not None:
+            st = G.lib().gpue_load_param_text(s._h, text.encode(), time_mode, None, None, 0)
+            assert st == 0, G.lib().gpue_last_error(s._h)
+        s.set_wfc(cases.initial_psi(c))
+        r = s.evolve(steps, gs, energy_every=c["energy_every"])
+        return s.get_wfc(), s.energy(), r
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _abi():
+    import gpue_b200 as G
+    G.lib().gpue_load_param_text.argtypes = [C.c_void_p, C.c_char_p, C.c_int32, C.c_void_p,
+                                              C.c_void_p, C.c_int32]
+    G.lib().gpue_load_param_text.restype = C.c_int
+
+
+def test_static_V_from_param_file_equals_the_harmonic_trap():
+    import gpue_b200 as G
+    c = dict(cases.DEFAULTS, dim=2, n=64, box=8.0, g=100.0, gsteps=200, seed=51, init="gauss",
+             wy=1.2, energy_every=100)
+    text = "V = 0.5*mass*((omegaX*x)*(omegaX*x)+(omegaY*y)*(omegaY*y))"
+    psi_f, E_f, _ = run(c, G.PREC_FP64, text)
+    psi_a, E_a, _ = run(c, G.PREC_FP64)
+    assert l2(psi_f, psi_a, c) <= 1e-12
+    assert abs(E_f - E_a) <= 1e-12 * abs(E_a)
+
+
+def test_static_gauge_and_V_with_appended_gauge_energy():
+    """V gets +0.5*mass*(Ax*Ax+Ay*Ay+Az*Az) appended when it is not last."""
+    import gpue_b200 as G
+    c = dict(cases.DEFAULTS, dim=2, n=64, box=8.0, g=150.0, omega=0.6, gauge=True, dt=5e-5,
+             esteps=120, seed=52, init="phase", energy_every=40)
+    text = ("Ax = 0-y*omega*omegaX\nAy = x*omega*omegaY\nAz = 0\n"
+            "V = 0.5*mass*((omegaX*x)*(omegaX*x)+(omegaY*y)*(omegaY*y))\nunused = 1")
+    psi_f, E_f, r_f = run(c, G.PREC_FP64, text)
+    # the oracle with the same fields as tables
+    asts, order, flags = ast_oracle.parse_param_text(text, doubles_for(c))
+    P = oracle_problem(c)
+    P.V[:] = find_field(ast_oracle.tree_to_array(asts["V"]), c)
+    P.Ax[:] = find_field(ast_oracle.tree_to_array(asts["Ax"]), c)
+    P.Ay[:] = find_field(ast_oracle.tree_to_array(asts["Ay"]), c)
+    psi0 = cases.initial_psi(c)
+    ref, res, en = P.evolve(psi0, c["esteps"], 1)
+    assert l2(psi_f, ref, c) <= 1e-12
+    Eref = P.energy(ref)
+    assert abs(E_f - Eref) <= 1e-12 * abs(Eref)
+    # and the same physics as the preset rotation gauge
+    psi_a, E_a, _ = run(c, G.PREC_FP64)
+    assert l2(psi_f, psi_a, c) <= 1e-11
+
+
+@pytest.mark.parametrize("gstate", [0, 1])
+def test_time_dependent_V_k_and_gauge(gstate):
+    """evolve()'s AST branches: V without the dt factor, k and V (linear) with
+    the full Dt, and the gauge multiplied by the raw A value, all evaluated at
+    (i dx, j dy, k dz, t)."""
+    import gpue_b200 as G
+    c = dict(cases.DEFAULTS, dim=2, n=64, box=8.0, g=80.0, gauge=True, omega=0.0, seed=53,
+             init="phase", energy_every=20, dt=5e-5, gdt=1e-4)
+    c["gsteps" if gstate == 0 else "esteps"] = 60
+    text = ("Ax = 1+0.001*sin(40*t)\n"
+            "k = 0.5*(x*x+y*y)*(1+0.1*cos(30*t))\n"
+            "V = 0.0002*(x+y)*(1+sin(50*t))")
+    psi_f, E_f, r_f = run(c, G.PREC_FP64, text, time_mode=1)
+    asts, order, flags = ast_oracle.parse_param_text(text, doubles_for(c))
+    assert {"Ax", "k", "V"} <= flags
+    P = oracle_problem(c)
+    P.V[:] = find_field(ast_oracle.tree_to_array(asts["V"]), c)
+    P.Ax[:] = find_field(ast_oracle.tree_to_array(asts["Ax"]), c)
+    for name, key in (("V", "V"), ("K", "k"), ("Ax", "Ax")):
+        P.set_ast(name, ast_oracle.tree_to_array(asts[key]))
+    psi0 = cases.initial_psi(c)
+    ref, res, en = P.evolve(psi0, 60, gstate)
+    assert l2(psi_f, ref, c) <= 1e-12
+    Eref = P.energy(ref)
+    assert abs(E_f - Eref) <= 1e-12 * abs(Eref)
+    psi32, E32, _ = run(c, G.PREC_FP32, text, time_mode=1)
+    assert abs(E32 - Eref) <= 1e-5 * abs(Eref)
+
+
+def test_bad_param_text_reports_an_ast_error():
+    import gpue_b200 as G
+    c = dict(cases.DEFAULTS, dim=2, n=32, box=6.0, seed=1, init="gauss", gsteps=1)
+    with G.Solver(product_params(c, G.PREC_FP64)) as s:
+        st = G.lib().gpue_load_param_text(s._h, b"V = nosuchname*x", 0, None, None, 0)
+        assert st == 5
+        assert b"nosuchname" in G.lib().gpue_last_error(s._h)
