@@ -1163,8 +1163,12 @@ gpue_status gpue_evolve(gpue_ctx* c, int32_t nsteps, int32_t gstate,
     if (o.no_sync && o.energy_calc_steps > 0)
         return fail(c, GPUE_ERR_INVALID_ARG, "no_sync excludes energy checks");
     const bool polish = o.polish_steps > 0 && c->prec == GPUE_PREC_FP32 && gstate == 0;
+    // the guard assumes a unitary real-time step; GPUE's time-dependent gauge
+    // multiplies by the raw A value, which is not, so the automatic choice
+    // leaves it off then
+    const bool unitary = c->prog_off[2] < 0 && c->prog_off[3] < 0 && c->prog_off[4] < 0;
     const bool guard = gstate == 1 && (o.norm_guard == 1 ||
-                                       (o.norm_guard < 0 && c->prec == GPUE_PREC_FP32));
+                                       (o.norm_guard < 0 && c->prec == GPUE_PREC_FP32 && unitary));
     gpue_status st = unpolish(c);
     if (st) return st;
     st = build_tables(c, c->prec, gstate);
