@@ -12,7 +12,8 @@ import os
 
 import numpy as np
 
-__all__ = ["lib", "Params", "EvolveOpts", "EvolveResult", "Solver", "GpueError",
+__all__ = ["lib", "Params", "EvolveOpts", "EvolveResult", "Solver", "GpueError", "Batch",
+           "BatchOpts", "BatchResult", "BatchStats",
            "PREC_FP64", "PREC_FP32", "C128", "C64", "MEM_HOST", "MEM_DEVICE",
            "GAUGE_ROTATION", "GAUGE_CONSTANT", "supported_length", "default_params"]
 
@@ -66,6 +67,28 @@ class EvolveResult(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("reserved")}
 
 
+class BatchOpts(C.Structure):
+    _fields_ = [("energy_calc_steps", C.c_int32), ("energy_calc_threshold", C.c_double),
+                ("threshold_abs", C.c_int32), ("max_steps", C.c_int32),
+                ("norm_guard", C.c_int32), ("segments_per_launch", C.c_int32),
+                ("reserved", C.c_int32 * 6)]
+
+
+class BatchResult(C.Structure):
+    _fields_ = [("steps_done", C.c_int32), ("early_stop", C.c_int32), ("energy", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("device_ms", C.c_double), ("kernel_launches", C.c_int64),
+                ("graph_launches", C.c_int64), ("point_steps", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -95,9 +118,21 @@ def lib():
         L.gpue_ctx_wfc_device.argtypes = [vp, C.POINTER(vp), C.POINTER(i32)]
         L.gpue_norm_noalloc.argtypes = [vp, i32, C.c_int64, C.c_double, vp, vp]
         L.gpue_norm_noalloc.restype = C.c_int
+        L.gpue_load_param_text.argtypes = [vp, C.c_char_p, i32, C.POINTER(C.c_char_p),
+                                           C.POINTER(C.c_double), i32]
+        L.gpue_ast_parse.argtypes = [C.c_char_p, C.POINTER(C.c_char_p), C.POINTER(C.c_double),
+                                     i32, vp, i32, C.POINTER(i32)]
+        L.gpue_batch_create.argtypes = [C.POINTER(vp), i32, C.POINTER(vp)]
+        L.gpue_batch_destroy.argtypes = [vp]
+        L.gpue_batch_last_error.argtypes = [vp]
+        L.gpue_batch_last_error.restype = C.c_char_p
+        L.gpue_batch_evolve.argtypes = [vp, i32, C.POINTER(BatchOpts), C.POINTER(BatchResult),
+                                        C.POINTER(BatchStats)]
         for name in ("gpue_default_params", "gpue_ctx_create", "gpue_ctx_destroy",
                      "gpue_set_operators", "gpue_set_wfc", "gpue_get_wfc", "gpue_evolve",
-                     "gpue_energy", "gpue_norm", "gpue_ctx_stream", "gpue_ctx_wfc_device"):
+                     "gpue_energy", "gpue_norm", "gpue_ctx_stream", "gpue_ctx_wfc_device",
+                     "gpue_load_param_text", "gpue_ast_parse", "gpue_batch_create",
+                     "gpue_batch_destroy", "gpue_batch_evolve"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -237,3 +272,58 @@ class Solver:
         p, d = C.c_void_p(), C.c_int32()
         self._ck(lib().gpue_ctx_wfc_device(self._h, C.byref(p), C.byref(d)))
         return p.value, d.value
+
+    def load_param_text(self, text, time_mode=0, doubles=None):
+        """Parameter-file fields (GPUE's -I file) from "name = expr" lines."""
+        doubles = doubles or {}
+        names = (C.c_char_p * max(1, len(doubles)))(*[k.encode() for k in doubles])
+        vals = (C.c_double * max(1, len(doubles)))(*doubles.values())
+        self._ck(lib().gpue_load_param_text(self._h, text.encode(), time_mode, names, vals,
+                                            len(doubles)))
+
+
+class Batch:
+    """Independent solves stepped together (gpue_batch_*); holds the Solvers."""
+
+    def __init__(self, solvers):
+        self.solvers = list(solvers)
+        arr = (C.c_void_p * len(self.solvers))(*[s._h.value for s in self.solvers])
+        h = C.c_void_p()
+        st = lib().gpue_batch_create(arr, len(self.solvers), C.byref(h))
+        if st != 0:
+            raise GpueError(st, "gpue_batch_create")
+        self._h = h
+
+    def close(self):
+        if self._h:
+            lib().gpue_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def evolve(self, gstate, max_steps, energy_every=0, threshold=-1.0, threshold_abs=False,
+               norm_guard=-1, segments_per_launch=0):
+        """Returns (per-solve result dicts, stats dict)."""
+        o = BatchOpts()
+        o.energy_calc_steps = energy_every
+        o.energy_calc_threshold = threshold
+        o.threshold_abs = 1 if threshold_abs else 0
+        o.max_steps = max_steps
+        o.norm_guard = norm_guard
+        o.segments_per_launch = segments_per_launch
+        res = (BatchResult * len(self.solvers))()
+        stats = BatchStats()
+        st = lib().gpue_batch_evolve(self._h, gstate, C.byref(o), res, C.byref(stats))
+        if st != 0:
+            raise GpueError(st, lib().gpue_batch_last_error(self._h).decode())
+        return [r.as_dict() for r in res], stats.as_dict()

@@ -77,7 +77,7 @@ __host__ __device__ inline double ast_apply(int op, double a, double b) {
 
 // Not inlined on the device: the pass kernels call it once per point from
 // fully unrolled loops, and one out-of-line copy keeps their code small.
-static __host__ __device__ __noinline__ double ast_eval(const AstInstr* prog, int n, double x,
+[[maybe_unused]] static __host__ __device__ __noinline__ double ast_eval(const AstInstr* prog, int n, double x,
                                                         double y, double z, double t) {
     double st[kAstMaxStack];
     int sp = 0;

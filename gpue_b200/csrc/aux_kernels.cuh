@@ -33,14 +33,12 @@ struct EnergyArgs {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_energy_real(const EnergyArgs a) {
-    __shared__ double scratch[16];
+__device__ __forceinline__ KSum energy_real_points(const EnergyArgs& a, long g0, long gstep) {
     const cx<T>* psi = reinterpret_cast<const cx<T>*>(a.psi);
     const double s = a.scale ? *a.scale : 1.0;
     const long nxy = (long)a.nx * a.ny;
     KSum acc{0.0, 0.0};
-    for (long g = (long)blockIdx.x * blockDim.x + threadIdx.x; g < a.N;
-         g += (long)gridDim.x * blockDim.x) {
+    for (long g = g0; g < a.N; g += gstep) {
         const int xi = (int)(g % a.nx);
         const int yi = (int)((g / a.nx) % a.ny);
         const int zi = (int)(g / nxy);
@@ -79,7 +77,90 @@ __global__ void __launch_bounds__(256) k_energy_real(const EnergyArgs a) {
         }
         acc.add(e);
     }
-    grid_reduce_finish(acc, scratch, a.red);
+    return acc;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_energy_real(const EnergyArgs a) {
+    __shared__ double scratch[16];
+    KSum acc = energy_real_points<T>(a, (long)blockIdx.x * blockDim.x + threadIdx.x,
+                                     (long)gridDim.x * blockDim.x);
+    grid_reduce_finish(acc, scratch, a.red, gridDim.x, blockIdx.x);
+}
+
+// Independent solves at once: `per` CTAs per solve, each solve reducing over
+// its own CTAs; converged solves (*active == 0) are skipped.
+template <typename T>
+__global__ void __launch_bounds__(256) k_energy_real_batch(const EnergyArgs* __restrict__ args,
+                                                          const int* const* __restrict__ active,
+                                                          int per) {
+    __shared__ double scratch[16];
+    const int s = blockIdx.x / per, b = blockIdx.x % per;
+    if (active[s] && *active[s] == 0) return;
+    const EnergyArgs& a = args[s];
+    KSum acc = energy_real_points<T>(a, (long)b * blockDim.x + threadIdx.x, (long)per * blockDim.x);
+    grid_reduce_finish(acc, scratch, a.red, per, b);
+}
+
+// Energy check of batched solves, one block.  Check k is taken after step
+// k*every (evolve's i % energy_calc_steps == 0 rule, src/evolution.cu:
+// 874-905), so a solve that stops there has run k*every + 1 steps.  E =
+// (ekin/N + ereal) dV; from the second check on, an imaginary-time solve
+// whose |E_previous - E| < threshold (absolute, or times E_previous) is
+// marked done.  *nactive receives the number of solves still running.
+struct CheckArgs {
+    double* scal;       // the solve's scalar slots
+    int* flags;         // [0] active, [1] steps done when it stopped
+    double inv_n;       // 1/N
+    double dV;
+    int slot_ekin, slot_ereal, slot_eold, slot_e;
+};
+
+__global__ void k_batch_check(const CheckArgs* __restrict__ args, int n, unsigned* nchecks,
+                              int every, double thr, int thr_abs, int can_stop, int* nactive) {
+    __shared__ unsigned k;
+    __shared__ int running;
+    if (threadIdx.x == 0) {
+        k = *nchecks;
+        running = 0;
+    }
+    __syncthreads();
+    for (int s = threadIdx.x; s < n; s += blockDim.x) {
+        const CheckArgs& c = args[s];
+        if (c.flags[0] == 0) continue;
+        const double E = (c.scal[c.slot_ekin] * c.inv_n + c.scal[c.slot_ereal]) * c.dV;
+        const double old = c.scal[c.slot_eold];
+        const bool stop = thr_abs ? fabs(old - E) < thr : fabs(old - E) < thr * old;
+        if (can_stop && k > 0 && stop) {
+            c.flags[0] = 0;
+            c.flags[1] = (int)k * every + 1;
+        } else {
+            atomicAdd(&running, 1);
+        }
+        c.scal[c.slot_eold] = E;
+        c.scal[c.slot_e] = E;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *nchecks = k + 1;
+        *nactive = running;
+    }
+}
+
+// One record per batched solve, gathered for a single device-to-host copy.
+struct BatchOut {
+    double energy;
+    int active;
+    int steps;
+};
+
+__global__ void k_batch_gather(const CheckArgs* __restrict__ args, int n, BatchOut* out) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const CheckArgs& c = args[s];
+        out[s].energy = c.scal[c.slot_e];
+        out[s].active = c.flags[0];
+        out[s].steps = c.flags[1];
+    }
 }
 
 // sum |psi|^2 (optionally times *scale^2) -> RED_SUM/RED_NORM
@@ -93,7 +174,7 @@ __global__ void __launch_bounds__(256) k_norm(const void* psi_, long N, RedArgs 
         const cx<T> v = psi[g];
         acc.add((double)v.x * v.x + (double)v.y * v.y);
     }
-    grid_reduce_finish(acc, scratch, red);
+    grid_reduce_finish(acc, scratch, red, gridDim.x, blockIdx.x);
 }
 
 template <typename T>

@@ -106,6 +106,7 @@ struct PassArgs {
     double step_dt;          // Dt
     double grid_d[3];        // dx, dy, dz as evolve() passes them (1 for absent axes)
     double hbar;
+    const int* active;       // batched solves: 0 once converged (skip the tiles)
 };
 
 // ------------------------------------------------------- FP64 reductions --
@@ -157,20 +158,22 @@ __device__ __forceinline__ KSum block_reduce(KSum k, double* scratch) {
 
 // Write this block's partial; the last block to arrive reduces all partials in
 // index order (deterministic) and writes the result.  All threads call it.
-__device__ __forceinline__ void grid_reduce_finish(KSum k, double* scratch, const RedArgs& a) {
+// nparts CTAs take part; this one writes partial `idx`.
+__device__ __forceinline__ void grid_reduce_finish(KSum k, double* scratch, const RedArgs& a,
+                                                   unsigned nparts, unsigned idx) {
     __shared__ unsigned s_last;
     k = block_reduce(k, scratch);
     if (threadIdx.x == 0) {
-        a.partials[blockIdx.x] = make_double2(k.s, k.c);
+        a.partials[idx] = make_double2(k.s, k.c);
         __threadfence();
         unsigned prev = atomicAdd(a.counter, 1u);
-        s_last = (prev == gridDim.x - 1) ? 1u : 0u;
+        s_last = (prev == nparts - 1) ? 1u : 0u;
     }
     __syncthreads();
     if (s_last) {
         __threadfence();
         KSum t{0.0, 0.0};
-        for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
+        for (unsigned i = threadIdx.x; i < nparts; i += blockDim.x) {
             double2 p = __ldcg(a.partials + i);
             t.merge(p.x, p.y);
         }
@@ -281,11 +284,13 @@ __device__ __forceinline__ cx<double> make_complex_ev(double v, int type) {
 }
 
 // EXT: also the table and expression forms of the factor ops.
+// Tiles t0, t0 + tstep, ... of one field; returns this thread's OP_NORM /
+// OP_EKIN accumulation.
 template <typename T, int N, int RA, int RB, int P, bool STRIDED, bool EXT>
-__global__ void __launch_bounds__(kMaxPassThreads, 2) k_pass(const PassArgs a) {
+__device__ __forceinline__ KSum pass_tiles(const PassArgs& a, long t0, long tstep,
+                                           unsigned char* smem_raw) {
     using L = LineFFT<T, N, RA, RB, P>;
     constexpr int E = L::E;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
 
     const int C = blockDim.x / P;
     int c, t;
@@ -307,7 +312,7 @@ __global__ void __launch_bounds__(kMaxPassThreads, 2) k_pass(const PassArgs a) {
     const long nxy = (long)a.nx * a.ny;
     KSum acc{0.0, 0.0};
 
-    for (long tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+    for (long tile = t0; tile < a.ntiles; tile += tstep) {
         const long line = tile * C + c;
         long base, stride;
         int xi = 0, yi = 0, zi = 0;  // line coordinates (the pass axis one is per element)
@@ -552,9 +557,44 @@ __global__ void __launch_bounds__(kMaxPassThreads, 2) k_pass(const PassArgs a) {
         }
     }
 
+    return acc;
+}
+
+// One field: a persistent grid walks the tiles.
+template <typename T, int N, int RA, int RB, int P, bool STRIDED, bool EXT>
+__global__ void __launch_bounds__(kMaxPassThreads, 2) k_pass(const PassArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    KSum acc = pass_tiles<T, N, RA, RB, P, STRIDED, EXT>(a, blockIdx.x, gridDim.x, smem_raw);
     if (a.red.kind != RED_NONE) {
         __syncthreads();  // smem is reused as reduction scratch
-        grid_reduce_finish(acc, reinterpret_cast<double*>(smem_raw), a.red);
+        grid_reduce_finish(acc, reinterpret_cast<double*>(smem_raw), a.red, gridDim.x,
+                           blockIdx.x);
+    }
+}
+
+// Many fields of the same length at once (independent solves): one CTA per
+// tile, tile_prefix[s] the first CTA of solve s.  A solve whose *active flag
+// is 0 (converged) is skipped; each solve reduces over its own tiles.
+template <typename T, int N, int RA, int RB, int P, bool STRIDED>
+__global__ void __launch_bounds__(kMaxPassThreads, 2)
+    k_pass_batch(const PassArgs* __restrict__ args, const long* __restrict__ tile_prefix,
+                 int nsolves) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const long b = blockIdx.x;
+    int lo = 0, hi = nsolves - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tile_prefix[mid] <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    const PassArgs& a = args[lo];
+    if (a.active && *a.active == 0) return;
+    const long tile = b - tile_prefix[lo];
+    KSum acc = pass_tiles<T, N, RA, RB, P, STRIDED, false>(a, tile, a.ntiles, smem_raw);
+    if (a.red.kind != RED_NONE) {
+        __syncthreads();
+        grid_reduce_finish(acc, reinterpret_cast<double*>(smem_raw), a.red,
+                           (unsigned)a.ntiles, (unsigned)tile);
     }
 }
 

