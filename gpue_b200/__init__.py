@@ -13,7 +13,8 @@ import os
 import numpy as np
 
 __all__ = ["lib", "Params", "EvolveOpts", "EvolveResult", "Solver", "GpueError", "Batch",
-           "BatchOpts", "BatchResult", "BatchStats",
+           "BatchOpts", "BatchResult", "BatchStats", "Server", "ServerOpts", "Request",
+           "ServerResult", "ServerStats",
            "PREC_FP64", "PREC_FP32", "C128", "C64", "MEM_HOST", "MEM_DEVICE",
            "GAUGE_ROTATION", "GAUGE_CONSTANT", "supported_length", "default_params"]
 
@@ -89,6 +90,39 @@ class BatchStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("device", C.c_int32), ("precision", C.c_int32),
+                ("hbm_budget_bytes", C.c_int64), ("check_steps", C.c_int32),
+                ("max_active", C.c_int32), ("threshold", C.c_double),
+                ("threshold_abs", C.c_int32), ("reserved", C.c_int32 * 7)]
+
+
+class Request(C.Structure):
+    _fields_ = [("params", Params), ("gstate", C.c_int32), ("max_steps", C.c_int32),
+                ("psi0", C.c_void_p), ("psi_out", C.c_void_p), ("tag", C.c_int64)]
+
+
+class ServerResult(C.Structure):
+    _fields_ = [("tag", C.c_int64), ("status", C.c_int32), ("steps_done", C.c_int32),
+                ("early_stop", C.c_int32), ("reserved0", C.c_int32), ("energy", C.c_double),
+                ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("reserved")}
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("admitted", C.c_int64), ("completed", C.c_int64),
+                ("failed", C.c_int64), ("active", C.c_int32), ("queued", C.c_int32),
+                ("bytes_resident", C.c_int64), ("bytes_peak", C.c_int64),
+                ("bytes_budget", C.c_int64), ("ticks", C.c_int64),
+                ("kernel_launches", C.c_int64), ("point_steps", C.c_double),
+                ("busy_s", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -128,6 +162,19 @@ def lib():
         L.gpue_batch_last_error.restype = C.c_char_p
         L.gpue_batch_evolve.argtypes = [vp, i32, C.POINTER(BatchOpts), C.POINTER(BatchResult),
                                         C.POINTER(BatchStats)]
+        L.gpue_server_create.argtypes = [C.POINTER(ServerOpts), C.POINTER(vp)]
+        L.gpue_server_destroy.argtypes = [vp]
+        L.gpue_server_last_error.argtypes = [vp]
+        L.gpue_server_last_error.restype = C.c_char_p
+        L.gpue_server_submit.argtypes = [vp, C.POINTER(Request)]
+        L.gpue_server_poll.argtypes = [vp, C.POINTER(ServerResult), i32, C.POINTER(i32),
+                                       C.c_double]
+        L.gpue_server_get_stats.argtypes = [vp, C.POINTER(ServerStats)]
+        L.gpue_server_clock.argtypes = [vp]
+        L.gpue_server_clock.restype = C.c_double
+        for name in ("gpue_server_create", "gpue_server_destroy", "gpue_server_submit",
+                     "gpue_server_poll", "gpue_server_get_stats"):
+            getattr(L, name).restype = C.c_int
         for name in ("gpue_default_params", "gpue_ctx_create", "gpue_ctx_destroy",
                      "gpue_set_operators", "gpue_set_wfc", "gpue_get_wfc", "gpue_evolve",
                      "gpue_energy", "gpue_norm", "gpue_ctx_stream", "gpue_ctx_wfc_device",
@@ -327,3 +374,85 @@ class Batch:
         if st != 0:
             raise GpueError(st, lib().gpue_batch_last_error(self._h).decode())
         return [r.as_dict() for r in res], stats.as_dict()
+
+
+class Server:
+    """The serving loop (gpue_server_*): submit solves, poll finished ones.
+
+    Each request's initial state (complex128) and, when asked for, its output
+    buffer are kept referenced here until its result has been polled."""
+
+    def __init__(self, precision=PREC_FP32, check_steps=100, threshold=1e-10,
+                 threshold_abs=True, hbm_budget=0, max_active=0, device=0):
+        o = ServerOpts()
+        o.device = device
+        o.precision = precision
+        o.hbm_budget_bytes = int(hbm_budget)
+        o.check_steps = check_steps
+        o.max_active = max_active
+        o.threshold = threshold
+        o.threshold_abs = 1 if threshold_abs else 0
+        h = C.c_void_p()
+        st = lib().gpue_server_create(C.byref(o), C.byref(h))
+        if st != 0:
+            raise GpueError(st, "gpue_server_create")
+        self._h = h
+        self._live = {}
+
+    def close(self):
+        if self._h:
+            lib().gpue_server_destroy(self._h)
+            self._h = None
+            self._live.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def submit(self, params, gstate, max_steps, psi0, tag, want_psi=True):
+        a = np.ascontiguousarray(psi0, dtype=np.complex128)
+        out = np.empty_like(a) if want_psi else None
+        q = Request()
+        q.params = params
+        q.gstate = gstate
+        q.max_steps = max_steps
+        q.psi0 = a.ctypes.data
+        q.psi_out = out.ctypes.data if out is not None else None
+        q.tag = tag
+        self._live[tag] = (a, out)
+        st = lib().gpue_server_submit(self._h, C.byref(q))
+        if st != 0:
+            del self._live[tag]
+            raise GpueError(st, lib().gpue_server_last_error(self._h).decode())
+
+    def poll(self, timeout=0.0, cap=256):
+        """Finished results as dicts (with "psi" when the output was kept)."""
+        buf = (ServerResult * cap)()
+        n = C.c_int32()
+        _check(lib().gpue_server_poll(self._h, buf, cap, C.byref(n), float(timeout)))
+        out = []
+        for i in range(n.value):
+            d = buf[i].as_dict()
+            a, psi = self._live.pop(d["tag"], (None, None))
+            d["psi"] = psi
+            out.append(d)
+        return out
+
+    def stats(self):
+        s = ServerStats()
+        lib().gpue_server_get_stats(self._h, C.byref(s))
+        return s.as_dict()
+
+    def clock(self):
+        return lib().gpue_server_clock(self._h)
+
+    def last_error(self):
+        return lib().gpue_server_last_error(self._h).decode()

@@ -102,49 +102,47 @@ __global__ void __launch_bounds__(256) k_energy_real_batch(const EnergyArgs* __r
     grid_reduce_finish(acc, scratch, a.red, per, b);
 }
 
-// Energy check of batched solves, one block.  Check k is taken after step
-// k*every (evolve's i % energy_calc_steps == 0 rule, src/evolution.cu:
-// 874-905), so a solve that stops there has run k*every + 1 steps.  E =
-// (ekin/N + ereal) dV; from the second check on, an imaginary-time solve
-// whose |E_previous - E| < threshold (absolute, or times E_previous) is
-// marked done.  *nactive receives the number of solves still running.
+// Energy check of batched solves, one block.  flags[2] counts a solve's
+// checks; check k (from 0) is taken after step k*every + step_base - 1, so
+// with step_base 1 the checks fall on evolve's i % energy_calc_steps == 0
+// steps (src/evolution.cu:872-905) and a solve that stops there has run
+// k*every + step_base steps.  E = (ekin/N + ereal) dV; from the second check
+// on, an imaginary-time solve whose |E_previous - E| < threshold (absolute,
+// or times E_previous) is marked done.  *nactive receives the number of
+// solves still running.
 struct CheckArgs {
     double* scal;       // the solve's scalar slots
-    int* flags;         // [0] active, [1] steps done when it stopped
+    int* flags;         // [0] active, [1] steps done when it stopped, [2] checks
     double inv_n;       // 1/N
     double dV;
     int slot_ekin, slot_ereal, slot_eold, slot_e;
 };
 
-__global__ void k_batch_check(const CheckArgs* __restrict__ args, int n, unsigned* nchecks,
-                              int every, double thr, int thr_abs, int can_stop, int* nactive) {
-    __shared__ unsigned k;
+static __global__ void k_batch_check(const CheckArgs* __restrict__ args, int n, int every,
+                              int step_base, double thr, int thr_abs, int can_stop,
+                              int* nactive) {
     __shared__ int running;
-    if (threadIdx.x == 0) {
-        k = *nchecks;
-        running = 0;
-    }
+    if (threadIdx.x == 0) running = 0;
     __syncthreads();
     for (int s = threadIdx.x; s < n; s += blockDim.x) {
         const CheckArgs& c = args[s];
         if (c.flags[0] == 0) continue;
+        const int k = c.flags[2];
         const double E = (c.scal[c.slot_ekin] * c.inv_n + c.scal[c.slot_ereal]) * c.dV;
         const double old = c.scal[c.slot_eold];
         const bool stop = thr_abs ? fabs(old - E) < thr : fabs(old - E) < thr * old;
         if (can_stop && k > 0 && stop) {
             c.flags[0] = 0;
-            c.flags[1] = (int)k * every + 1;
+            c.flags[1] = k * every + step_base;
         } else {
             atomicAdd(&running, 1);
         }
+        c.flags[2] = k + 1;
         c.scal[c.slot_eold] = E;
         c.scal[c.slot_e] = E;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        *nchecks = k + 1;
-        *nactive = running;
-    }
+    if (threadIdx.x == 0) *nactive = running;
 }
 
 // One record per batched solve, gathered for a single device-to-host copy.
@@ -152,14 +150,18 @@ struct BatchOut {
     double energy;
     int active;
     int steps;
+    int checks;
+    int pad;
 };
 
-__global__ void k_batch_gather(const CheckArgs* __restrict__ args, int n, BatchOut* out) {
+static __global__ void k_batch_gather(const CheckArgs* __restrict__ args, int n, BatchOut* out) {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
         const CheckArgs& c = args[s];
         out[s].energy = c.scal[c.slot_e];
         out[s].active = c.flags[0];
         out[s].steps = c.flags[1];
+        out[s].checks = c.flags[2];
+        out[s].pad = 0;
     }
 }
 

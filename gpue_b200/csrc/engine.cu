@@ -21,129 +21,13 @@
 // steps that end an imaginary-time run; after a polish the FP64 state is the
 // authoritative one until the next FP32 evolve.
 
-#include <cuda_runtime.h>
 
-#include <algorithm>
-#include <cctype>
-#include <cmath>
-#include <cstdarg>
-#include <cstdio>
-#include <cstring>
-#include <functional>
-#include <map>
-#include <memory>
-#include <string>
-#include <vector>
-
-#include "../../include/gpue_b200.h"
-#include "ast.h"
-#include "aux_kernels.cuh"
-#include "registry.h"
+#include "engine_internal.h"
 
 using namespace gpue;
+using namespace gpue_eng;
 
-namespace {
-
-const double kPI = 3.141592653589793;  // GPUE's PI (include/constants.h)
-
-struct Axis {
-    int n = 1;
-    double xmax = 0, dx = 1;
-    std::vector<double> x, p;  // positions, momenta (generate_p_space order)
-};
-
-// Device tables for one precision.
-struct Tables {
-    void* buf = nullptr;
-    const double2* vfac[3] = {};
-    const double2* kfac[3] = {};
-    const void* tw[3] = {};
-    const double* pos[3] = {};
-    const double* mom[3] = {};
-    const double* vreal[3] = {};
-    int built_for = -1;  // gstate of vfac/kfac
-};
-
-struct LaunchCfg {
-    const PassKernel* k = nullptr;
-    int threads = 0, blocks = 0;
-    long ntiles = 0;
-    size_t smem = 0;
-};
-
-struct GraphKey {
-    int prec, gstate, parity, nsteps, scale_first, energy_last, guard;
-    bool operator<(const GraphKey& o) const {
-        return std::memcmp(this, &o, sizeof(GraphKey)) < 0;
-    }
-};
-
-struct Segment {
-    cudaGraphExec_t exec = nullptr;
-    long launches = 0;
-};
-
-}  // namespace
-
-struct gpue_ctx {
-    gpue_params p{};
-    int dim = 2;
-    int prec = GPUE_PREC_FP64;
-    Axis ax[3];
-    long N = 0;
-    double dV = 1;
-    int device = 0;
-    int sms = 148;
-    cudaStream_t stream = nullptr;
-    void* psi = nullptr;      // resident state in the context precision
-    void* psi64 = nullptr;    // FP64 shadow of an FP32 context (polishing)
-    bool polished = false;    // psi64 holds the authoritative state
-    void* scratch = nullptr;  // N * 16 bytes
-    double* scal = nullptr;   // device scalars
-    double2* partials = nullptr;
-    long partials_cap = 0;
-    unsigned* counters = nullptr;
-    int* dflags = nullptr;       // [0] active (batched runs), [1] steps when converged
-    Tables tab[2];            // indexed by GPUE_PREC_*
-    LaunchCfg lc[2][3];       // [precision][axis]
-    bool have_wfc = false;
-    bool pending_scale = false;  // scal[kScale] must multiply psi
-    std::map<GraphKey, Segment> graphs;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    std::string err;
-    long launches = 0;         // kernels enqueued in the current evolve call
-    double last_energy = 0.0;  // energy of the latest check (GPUE's "energy" key)
-    // parameter-file fields (gpue_load_param_text)
-    bool ext = false;          // passes use the table / expression forms
-    double* vtab = nullptr;    // static V(g) and A_a(g) (FP64, N each)
-    double* atab[3] = {};
-    bool use_atab = false;     // gauge from the A tables instead of the rotation preset
-    bool atab_nonzero[3] = {};
-    AstInstr* progs = nullptr; // device copy of the time-dependent programs
-    int prog_off[5] = {-1, -1, -1, -1, -1};  // V, k, Ax, Ay, Az
-    int prog_len[5] = {};
-    bool time_dep = false;     // some factor is evaluated per step
-};
-
-namespace {
-
-// device scalar slots
-enum {
-    kScale = 0,       // imaginary-time renormalisation factor
-    kEkin = 1,
-    kEreal = 2,
-    kNorm = 3,
-    kGuard = 4,       // real-time norm-guard factor
-    kTargetImag = 5,  // 1/dV: sum |psi|^2 of a unit-norm state
-    kTargetReal = 6,  // sum |psi|^2 at the start of a real-time evolve
-    kOne = 7,
-    kEold = 8,        // batched runs: energy of the previous check
-    kEcheck = 9,      // batched runs: energy of the latest check
-    kNScal = 16
-};
-// counter slots: reductions in flight in one stream use distinct counters
-enum { kCtrNorm = 0, kCtrEkin = 1, kCtrEreal = 2, kCtrMisc = 3, kNCtr = 8 };
-constexpr long kAuxPartials = 4096;  // partials reserved for the aux kernels
+namespace gpue_eng {
 
 gpue_status fail(gpue_ctx* c, gpue_status st, const char* fmt, ...) {
     if (c) {
@@ -156,16 +40,6 @@ gpue_status fail(gpue_ctx* c, gpue_status st, const char* fmt, ...) {
     }
     return st;
 }
-
-#define CK(call)                                                                         \
-    do {                                                                                 \
-        cudaError_t e_ = (call);                                                         \
-        if (e_ != cudaSuccess)                                                           \
-            return fail(c, e_ == cudaErrorMemoryAllocation ? GPUE_ERR_OUT_OF_MEMORY      \
-                                                           : GPUE_ERR_CUDA,              \
-                        "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__,       \
-                        __LINE__);                                                       \
-    } while (0)
 
 size_t elem_size(int prec) { return prec == GPUE_PREC_FP32 ? 8 : 16; }
 int kprec(int prec) { return prec == GPUE_PREC_FP32 ? PREC_F32 : PREC_F64; }
@@ -358,22 +232,6 @@ gpue_status plan_axis(gpue_ctx* c, int prec, int axis) {
     return GPUE_OK;
 }
 
-struct LPass {
-    int axis = 0;
-    std::vector<int> ops;
-    int red = RED_NONE;       // RED_NONE / RED_NORM / RED_SUM
-    bool red_blocks = true;   // the next pass needs the reduction result
-    int red_slot = 0;         // scalar slot for the result
-    int red_target = kTargetImag;
-    int ctr = 0;              // counter slot
-    bool store = true;
-    bool to_scratch = false;   // out = scratch
-    bool from_scratch = false; // in = scratch
-    double gauge_dt = 0;       // for OP_GAUGE
-    int scale_slot = kScale;   // OP_SCALE factor
-    int kscale_slot = -1;      // extra factor folded into OP_KPHASE (norm guard)
-    double time = 0;           // Dt * step, for time-dependent expressions
-};
 
 gpue_status make_pass_args(gpue_ctx* c, int prec, const LPass& lp, int gstate, PassArgs& a) {
     const LaunchCfg& lc = c->lc[prec][lp.axis];
@@ -815,6 +673,35 @@ gpue_status step_loop(gpue_ctx* c, int prec, int off, int nsteps, int gstate,
     return GPUE_OK;
 }
 
+size_t ctx_bytes_estimate(int dim, int n, int prec) {
+    auto al = [](size_t b) { return ((b + 255) / 256) * 256; };
+    const size_t N = (size_t)n * n * (dim == 3 ? n : 1);
+    const size_t cap = N / n + kAuxPartials + 1024;  // partials_cap (gpue_ctx_create)
+    size_t b = al(N * elem_size(prec)) + al(N * 16);  // state, scratch
+    b += al(kNScal * sizeof(double)) + al(cap * sizeof(double2)) +
+         al(kNCtr * sizeof(unsigned)) + al(4 * sizeof(int));
+    const size_t tn = 3 * (2 * al((size_t)n * 16) + al((size_t)n * elem_size(prec)) +
+                           3 * al((size_t)n * 8));
+    return b + tn;  // one precision's operator tables
+}
+
+size_t ctx_device_bytes(const gpue_ctx* c) {
+    auto al = [](size_t b) { return ((b + 255) / 256) * 256; };
+    size_t b = ctx_bytes_estimate(c->dim, c->ax[0].n, c->prec);
+    if (c->psi64) b += al(c->N * 16);  // FP64 shadow
+    if (c->tab[1 - c->prec].buf) {
+        const int o = 1 - c->prec;
+        for (int a = 0; a < 3; ++a) {
+            const size_t n = c->ax[a].n;
+            b += 2 * al(n * 16) + al(n * elem_size(o)) + 3 * al(n * 8);
+        }
+    }
+    if (c->vtab) b += al(c->N * 8);
+    for (auto t : c->atab)
+        if (t) b += al(c->N * 8);
+    return b;
+}
+
 gpue_status ensure_shadow(gpue_ctx* c) {
     if (c->psi64) return GPUE_OK;
     CK(cudaMalloc(&c->psi64, c->N * 16));
@@ -834,7 +721,7 @@ gpue_status unpolish(gpue_ctx* c) {
     return GPUE_OK;
 }
 
-}  // namespace
+}  // namespace gpue_eng
 
 // ================================================================= C ABI ==
 
@@ -1260,549 +1147,6 @@ gpue_status gpue_evolve(gpue_ctx* c, int32_t nsteps, int32_t gstate,
         st = norm_now(c, c->polished ? GPUE_PREC_FP64 : c->prec, &nrm);
         if (st) return st;
         res->norm = nrm;
-    }
-    return GPUE_OK;
-}
-
-}  // extern "C"
-
-// =============================================================== batches ==
-//
-// A batch runs many contexts' imaginary- or real-time steps together.  Its
-// solves are grouped by (precision, dimension, grid, launch shape, pass
-// schedule); a group issues one k_pass_batch launch per logical pass over all
-// its members' tiles, each CTA finding its solve in a prefix table.  Groups
-// run on their own streams between a fork and a join; after the join one
-// block evaluates every solve's energy check and clears the active flag of
-// those that stopped, which freezes them for the rest of the run.  The run
-// is cut into segments that end after each check step and replayed as CUDA
-// graphs; kernel argument arrays live in device chunks owned by the batch.
-
-struct gpue_batch {
-    std::vector<gpue_ctx*> ctx;
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
-    cudaEvent_t polled[2] = {nullptr, nullptr};
-    std::vector<cudaStream_t> lanes;
-    std::vector<cudaEvent_t> joins;
-    std::vector<std::pair<char*, size_t>> chunks;  // device argument storage
-    size_t chunk_used = 0;
-    std::map<std::string, const void*> stored;
-    CheckArgs* checks = nullptr;  // device, one per solve
-    BatchOut* outs = nullptr;     // device
-    BatchOut* h_outs = nullptr;   // pinned
-    unsigned* nchecks = nullptr;
-    int* nactive = nullptr;       // device, two slots (alternating polls)
-    int* h_nactive = nullptr;     // pinned, two slots
-    std::map<std::string, Segment> graphs;
-    std::string err;
-};
-
-namespace {
-
-gpue_status bfail(gpue_batch* b, gpue_status st, const char* fmt, ...) {
-    if (b) {
-        char buf[512];
-        va_list ap;
-        va_start(ap, fmt);
-        vsnprintf(buf, sizeof buf, fmt, ap);
-        va_end(ap);
-        b->err = buf;
-    }
-    return st;
-}
-
-#define BCK(call)                                                                        \
-    do {                                                                                 \
-        cudaError_t e_ = (call);                                                         \
-        if (e_ != cudaSuccess)                                                           \
-            return bfail(b, e_ == cudaErrorMemoryAllocation ? GPUE_ERR_OUT_OF_MEMORY     \
-                                                            : GPUE_ERR_CUDA,             \
-                         "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__,      \
-                         __LINE__);                                                      \
-    } while (0)
-
-// a context error surfaces as the batch error
-#define BCTX(c, call)                                    \
-    do {                                                 \
-        gpue_status s_ = (call);                         \
-        if (s_) {                                        \
-            b->err = (c)->err;                           \
-            return s_;                                   \
-        }                                                \
-    } while (0)
-
-struct BGroup {
-    int prec = 0;
-    bool guard = false;
-    std::vector<int> members;
-};
-
-// Copies an argument array to device memory once; equal arrays share storage.
-gpue_status bstore(gpue_batch* b, const void* data, size_t bytes, const void** out) {
-    std::string key(static_cast<const char*>(data), bytes);
-    auto it = b->stored.find(key);
-    if (it != b->stored.end()) {
-        *out = it->second;
-        return GPUE_OK;
-    }
-    const size_t need = (bytes + 255) & ~size_t(255);
-    if (b->chunks.empty() || b->chunk_used + need > b->chunks.back().second) {
-        const size_t cap = std::max<size_t>(size_t(4) << 20, need);
-        char* p = nullptr;
-        BCK(cudaMalloc(&p, cap));
-        b->chunks.emplace_back(p, cap);
-        b->chunk_used = 0;
-    }
-    char* dst = b->chunks.back().first + b->chunk_used;
-    BCK(cudaMemcpy(dst, data, bytes, cudaMemcpyHostToDevice));
-    b->chunk_used += need;
-    b->stored.emplace(std::move(key), dst);
-    *out = dst;
-    return GPUE_OK;
-}
-
-// Passes of steps [i0, i1) of one solve as the batch issues them.
-std::vector<LPass> batch_passes(gpue_ctx* c, int i0, int i1, int gstate, bool guard) {
-    std::vector<LPass> v;
-    for (int i = i0; i < i1; ++i)
-        step_passes(c, i, gstate, gstate == 0 && i > 0, 1.0, guard, v);
-    fuse(v);
-    return v;
-}
-
-// Solves with equal signatures can share launches.
-std::string batch_signature(gpue_ctx* c, int gstate, bool guard) {
-    std::string s;
-    auto put = [&](long x) { s += std::to_string(x) + ","; };
-    put(c->prec);
-    put(c->dim);
-    for (int a = 0; a < c->dim; ++a) {
-        const LaunchCfg& lc = c->lc[c->prec][a];
-        put(c->ax[a].n);
-        put(lc.threads);
-        put(lc.ntiles);
-        put((long)lc.smem);
-    }
-    for (const LPass& lp : batch_passes(c, 0, 3, gstate, guard)) {
-        s += "|";
-        put(lp.axis);
-        for (int op : lp.ops) put(op);
-        put(lp.red);
-        put(lp.red_blocks);
-        put(lp.red_slot);
-        put(lp.red_target);
-        put(lp.ctr);
-        put(lp.store);
-        put(lp.to_scratch);
-        put(lp.from_scratch);
-        put(lp.scale_slot);
-        put(lp.kscale_slot);
-    }
-    return s;
-}
-
-using LaunchOp = std::function<void(cudaStream_t)>;
-
-struct SegPlan {
-    std::vector<std::vector<LaunchOp>> lanes;  // one list per group
-    bool check = false;
-    long launches = 0;
-};
-
-struct BatchRun {
-    int gstate = 0;
-    int every = 0;
-    double thr = 0;
-    int thr_abs = 0;
-    std::vector<BGroup> groups;
-};
-
-gpue_status set_batch_smem(gpue_batch* b, const void* fn, size_t smem) {
-    if (smem > 48 * 1024)
-        BCK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    return GPUE_OK;
-}
-
-// Builds the launches of one segment [i0, i1) (+ energy and check).
-gpue_status plan_segment(gpue_batch* b, const BatchRun& r, int i0, int i1, bool check,
-                         SegPlan& sp) {
-    sp.lanes.assign(r.groups.size(), {});
-    sp.check = check;
-    for (size_t gi = 0; gi < r.groups.size(); ++gi) {
-        const BGroup& g = r.groups[gi];
-        const int n = (int)g.members.size();
-        gpue_ctx* c0 = b->ctx[g.members[0]];
-        std::vector<std::vector<LPass>> lists(n);
-        for (int k = 0; k < n; ++k)
-            lists[k] = batch_passes(b->ctx[g.members[k]], i0, i1, r.gstate, g.guard);
-        if (check)
-            for (int k = 0; k < n; ++k)
-                for (const LPass& lp : energy_passes(b->ctx[g.members[k]], r.gstate == 0))
-                    lists[k].push_back(lp);
-        const size_t npass = lists[0].size();
-        std::vector<PassArgs> args(n);
-        std::vector<long> prefix(n);
-        for (size_t j = 0; j < npass; ++j) {
-            const int axis = lists[0][j].axis;
-            for (int k = 0; k < n; ++k) {
-                gpue_ctx* c = b->ctx[g.members[k]];
-                if (lists[k].size() != npass || lists[k][j].axis != axis)
-                    return bfail(b, GPUE_ERR_STATE, "batch group schedules differ");
-                BCTX(c, make_pass_args(c, g.prec, lists[k][j], r.gstate, args[k]));
-            }
-            const LaunchCfg& lc = c0->lc[g.prec][axis];
-            for (int k = 0; k < n; ++k) prefix[k] = (long)k * lc.ntiles;
-            const void *dargs, *dprefix;
-            gpue_status st = bstore(b, args.data(), n * sizeof(PassArgs), &dargs);
-            if (st) return st;
-            st = bstore(b, prefix.data(), n * sizeof(long), &dprefix);
-            if (st) return st;
-            void (*fn)(const PassArgs*, const long*, int) =
-                axis == 0 ? lc.k->row_batch : lc.k->col_batch;
-            st = set_batch_smem(b, (const void*)fn, lc.smem);
-            if (st) return st;
-            const unsigned grid = (unsigned)(n * lc.ntiles);
-            const unsigned threads = (unsigned)lc.threads;
-            const size_t smem = lc.smem;
-            sp.lanes[gi].push_back([=](cudaStream_t s) {
-                fn<<<grid, threads, smem, s>>>(static_cast<const PassArgs*>(dargs),
-                                               static_cast<const long*>(dprefix), n);
-            });
-            sp.launches++;
-        }
-        if (check) {
-            std::vector<EnergyArgs> ea(n);
-            std::vector<const int*> act(n);
-            for (int k = 0; k < n; ++k) {
-                gpue_ctx* c = b->ctx[g.members[k]];
-                ea[k] = energy_args(c, g.prec, r.gstate == 0);
-                act[k] = c->dflags;
-            }
-            const void *dea, *dact;
-            gpue_status st = bstore(b, ea.data(), n * sizeof(EnergyArgs), &dea);
-            if (st) return st;
-            st = bstore(b, act.data(), n * sizeof(const int*), &dact);
-            if (st) return st;
-            long per = c0->N / (256 * 8);
-            per = std::max(1L, std::min(per, kAuxPartials));
-            const unsigned grid = (unsigned)(n * per);
-            const int iper = (int)per;
-            const bool f32 = g.prec == GPUE_PREC_FP32;
-            sp.lanes[gi].push_back([=](cudaStream_t s) {
-                const EnergyArgs* e = static_cast<const EnergyArgs*>(dea);
-                const int* const* a = static_cast<const int* const*>(dact);
-                if (f32) k_energy_real_batch<float><<<grid, 256, 0, s>>>(e, a, iper);
-                else k_energy_real_batch<double><<<grid, 256, 0, s>>>(e, a, iper);
-            });
-            sp.launches++;
-        }
-    }
-    if (check) sp.launches++;  // k_batch_check
-    return GPUE_OK;
-}
-
-// Captures a list of segments into one graph.
-gpue_status capture_segments(gpue_batch* b, const BatchRun& r, const std::vector<SegPlan>& segs,
-                             Segment& out) {
-    while (b->lanes.size() < r.groups.size()) {
-        cudaStream_t s;
-        cudaEvent_t e;
-        BCK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-        BCK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        b->lanes.push_back(s);
-        b->joins.push_back(e);
-    }
-    BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    const int n = (int)b->ctx.size();
-    int* nact = b->nactive;
-    const CheckArgs* checks = b->checks;
-    unsigned* nchecks = b->nchecks;
-    long launches = 0;
-    for (const SegPlan& sp : segs) {
-        cudaEventRecord(b->fork, b->stream);
-        for (size_t gi = 0; gi < sp.lanes.size(); ++gi) {
-            cudaStream_t s = b->lanes[gi];
-            cudaStreamWaitEvent(s, b->fork, 0);
-            for (const LaunchOp& op : sp.lanes[gi]) op(s);
-            cudaEventRecord(b->joins[gi], s);
-            cudaStreamWaitEvent(b->stream, b->joins[gi], 0);
-        }
-        if (sp.check)
-            k_batch_check<<<1, 256, 0, b->stream>>>(checks, n, nchecks, r.every, r.thr, r.thr_abs,
-                                                    r.gstate == 0 ? 1 : 0, nact);
-        launches += sp.launches;
-    }
-    cudaGraph_t g = nullptr;
-    cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
-    BCK(ce);
-    BCK(cudaGetLastError());
-    ce = cudaGraphInstantiate(&out.exec, g, 0);
-    cudaGraphDestroy(g);
-    BCK(ce);
-    out.launches = launches;
-    return GPUE_OK;
-}
-
-struct SegSpec {
-    int i0, i1;
-    bool check;
-};
-
-// GPUE's schedule cut into segments: a check after step k*every (k >= 0)
-// ends a segment; unchecked stretches are cut into at most `chunk` steps.
-std::vector<SegSpec> batch_schedule(int nsteps, int every, int chunk) {
-    std::vector<SegSpec> v;
-    int i = 0;
-    while (i < nsteps) {
-        int end = std::min(nsteps, i + chunk);
-        bool check = false;
-        if (every > 0) {
-            const int nc = ((i + every - 1) / every) * every;  // next check step >= i
-            if (nc < nsteps && nc + 1 <= end) {
-                end = nc + 1;
-                check = true;
-            }
-        }
-        v.push_back({i, end, check});
-        i = end;
-    }
-    return v;
-}
-
-void destroy_batch_graphs(gpue_batch* b) {
-    for (auto& kv : b->graphs)
-        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-    b->graphs.clear();
-}
-
-}  // namespace
-
-extern "C" {
-
-const char* gpue_batch_last_error(const gpue_batch* b) { return b ? b->err.c_str() : ""; }
-
-gpue_status gpue_batch_create(gpue_ctx* const* ctxs, int32_t n, gpue_batch** out) {
-    if (!ctxs || n < 1 || !out) return GPUE_ERR_INVALID_ARG;
-    *out = nullptr;
-    for (int i = 0; i < n; ++i) {
-        if (!ctxs[i] || ctxs[i]->device != ctxs[0]->device) return GPUE_ERR_INVALID_ARG;
-        for (int j = 0; j < i; ++j)
-            if (ctxs[j] == ctxs[i]) return GPUE_ERR_INVALID_ARG;
-    }
-    std::unique_ptr<gpue_batch> bp(new gpue_batch);
-    gpue_batch* b = bp.get();
-    b->ctx.assign(ctxs, ctxs + n);
-    b->device = ctxs[0]->device;
-    BCK(cudaSetDevice(b->device));
-    BCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-    BCK(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
-    BCK(cudaEventCreate(&b->ev0));
-    BCK(cudaEventCreate(&b->ev1));
-    for (auto& e : b->polled) BCK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    BCK(cudaMalloc(&b->checks, n * sizeof(CheckArgs)));
-    BCK(cudaMalloc(&b->outs, n * sizeof(BatchOut)));
-    BCK(cudaMallocHost(&b->h_outs, n * sizeof(BatchOut)));
-    BCK(cudaMalloc(&b->nchecks, sizeof(unsigned)));
-    BCK(cudaMalloc(&b->nactive, 2 * sizeof(int)));
-    BCK(cudaMallocHost(&b->h_nactive, 2 * sizeof(int)));
-    std::vector<CheckArgs> h(n);
-    for (int i = 0; i < n; ++i) {
-        gpue_ctx* c = ctxs[i];
-        h[i].scal = c->scal;
-        h[i].flags = c->dflags;
-        h[i].inv_n = 1.0 / (double)c->N;
-        h[i].dV = c->dV;
-        h[i].slot_ekin = kEkin;
-        h[i].slot_ereal = kEreal;
-        h[i].slot_eold = kEold;
-        h[i].slot_e = kEcheck;
-    }
-    BCK(cudaMemcpy(b->checks, h.data(), n * sizeof(CheckArgs), cudaMemcpyHostToDevice));
-    *out = bp.release();
-    return GPUE_OK;
-}
-
-gpue_status gpue_batch_destroy(gpue_batch* b) {
-    if (!b) return GPUE_OK;
-    cudaSetDevice(b->device);
-    if (b->stream) cudaStreamSynchronize(b->stream);
-    destroy_batch_graphs(b);
-    for (auto& ch : b->chunks) cudaFree(ch.first);
-    for (auto s : b->lanes) cudaStreamDestroy(s);
-    for (auto e : b->joins) cudaEventDestroy(e);
-    cudaFree(b->checks);
-    cudaFree(b->outs);
-    cudaFreeHost(b->h_outs);
-    cudaFree(b->nchecks);
-    cudaFree(b->nactive);
-    cudaFreeHost(b->h_nactive);
-    for (auto e : {b->fork, b->ev0, b->ev1, b->polled[0], b->polled[1]})
-        if (e) cudaEventDestroy(e);
-    if (b->stream) cudaStreamDestroy(b->stream);
-    delete b;
-    return GPUE_OK;
-}
-
-gpue_status gpue_batch_evolve(gpue_batch* b, int32_t gstate, const gpue_batch_opts* opts,
-                              gpue_batch_result* results, gpue_batch_stats* stats) {
-    if (!b || (gstate != 0 && gstate != 1)) return GPUE_ERR_INVALID_ARG;
-    gpue_batch_opts o;
-    std::memset(&o, 0, sizeof o);
-    o.norm_guard = -1;
-    o.max_steps = 1;
-    if (opts) o = *opts;
-    if (o.max_steps < 1 || o.energy_calc_steps < 0 || o.segments_per_launch < 0)
-        return bfail(b, GPUE_ERR_INVALID_ARG, "invalid batch options");
-    BCK(cudaSetDevice(b->device));
-    const int n = (int)b->ctx.size();
-    BatchRun r;
-    r.gstate = gstate;
-    r.every = o.energy_calc_steps;
-    r.thr = o.energy_calc_threshold;
-    r.thr_abs = o.threshold_abs ? 1 : 0;
-    std::map<std::string, int> by_sig;
-    std::string gkey = std::to_string(gstate) + ":" + std::to_string(r.every) + ":" +
-                       std::to_string(r.thr_abs) + ":";
-    {
-        char tb[32];
-        std::snprintf(tb, sizeof tb, "%a:", r.thr);
-        gkey += tb;
-    }
-    double pts = 0;
-    const int one[4] = {1, 0, 0, 0};
-    for (int i = 0; i < n; ++i) {
-        gpue_ctx* c = b->ctx[i];
-        if (!c->have_wfc) return bfail(b, GPUE_ERR_STATE, "solve %d has no wavefunction", i);
-        if (c->ext)
-            return bfail(b, GPUE_ERR_UNSUPPORTED, "solve %d: parameter-file fields are not batched", i);
-        if (c->p.ramp && gstate == 0 && c->p.corotating &&
-            (axis_gauge_active(c, 0) || axis_gauge_active(c, 1) || axis_gauge_active(c, 2)))
-            return bfail(b, GPUE_ERR_UNSUPPORTED, "solve %d: the ramp is not batched", i);
-        const bool guard = gstate == 1 && (o.norm_guard == 1 ||
-                                           (o.norm_guard < 0 && c->prec == GPUE_PREC_FP32));
-        BCTX(c, unpolish(c));
-        BCTX(c, build_tables(c, c->prec, gstate));
-        BCTX(c, apply_pending_scale(c, c->prec));
-        if (guard) {
-            BCTX(c, norm_to_slot(c, c->prec, kTargetReal));
-            BCK(cudaMemcpyAsync(c->scal + kGuard, c->scal + kOne, sizeof(double),
-                                cudaMemcpyDeviceToDevice, c->stream));
-        }
-        BCK(cudaMemcpyAsync(c->dflags, one, sizeof one, cudaMemcpyHostToDevice, c->stream));
-        BCK(cudaStreamSynchronize(c->stream));
-        const std::string sig = std::to_string(guard) + "/" + batch_signature(c, gstate, guard);
-        auto it = by_sig.find(sig);
-        if (it == by_sig.end()) {
-            it = by_sig.emplace(sig, (int)r.groups.size()).first;
-            BGroup g;
-            g.prec = c->prec;
-            g.guard = guard;
-            r.groups.push_back(g);
-        }
-        r.groups[it->second].members.push_back(i);
-        if (r.groups[it->second].members.size() == 1) gkey += "{" + sig + "}";
-        gkey += std::to_string(it->second) + ",";
-        pts += (double)c->N;
-    }
-    BCK(cudaMemsetAsync(b->nchecks, 0, sizeof(unsigned), b->stream));
-    const int every = r.every;
-    const std::vector<SegSpec> sched = batch_schedule(o.max_steps, every, every > 0 ? std::min(every + 1, 256) : 128);
-    int per_launch = o.segments_per_launch;
-    if (per_launch == 0) {
-        // about 2e9 point-steps per graph launch, at most 16 segments
-        const double seg_work = pts * (every > 0 ? every : 128);
-        per_launch = (int)std::min(16.0, std::max(1.0, std::ceil(2e9 / seg_work)));
-    }
-    long launches = 0, glaunches = 0;
-    int steps_run = 0, polls = 0;
-    bool all_done = false;
-    BCK(cudaEventRecord(b->ev0, b->stream));
-    size_t s = 0;
-    while (s < sched.size() && !all_done) {
-        // consecutive segments of equal shape share one graph launch
-        size_t e = s + 1;
-        while (e < sched.size() && (int)(e - s) < per_launch && sched[s].i0 > 0 &&
-               sched[e].i1 - sched[e].i0 == sched[s].i1 - sched[s].i0 &&
-               sched[e].check == sched[s].check)
-            ++e;
-        std::string key = gkey + "#" + std::to_string(sched[s].i0 == 0) + "," +
-                          std::to_string(sched[s].i0 % 2);
-        bool has_check = false;
-        for (size_t k = s; k < e; ++k) {
-            key += ";" + std::to_string(sched[k].i1 - sched[k].i0) + (sched[k].check ? "c" : "");
-            has_check |= sched[k].check;
-        }
-        auto it = b->graphs.find(key);
-        if (it == b->graphs.end()) {
-            std::vector<SegPlan> plans(e - s);
-            for (size_t k = s; k < e; ++k) {
-                gpue_status st = plan_segment(b, r, sched[k].i0, sched[k].i1, sched[k].check,
-                                              plans[k - s]);
-                if (st) return st;
-            }
-            Segment seg;
-            gpue_status st = capture_segments(b, r, plans, seg);
-            if (st) return st;
-            it = b->graphs.emplace(key, seg).first;
-        }
-        BCK(cudaGraphLaunch(it->second.exec, b->stream));
-        glaunches++;
-        launches += it->second.launches;
-        steps_run = sched[e - 1].i1;
-        if (has_check && gstate == 0) {
-            // poll the previous launch's count while this one runs
-            const int slot = polls % 2;
-            BCK(cudaMemcpyAsync(b->h_nactive + slot, b->nactive, sizeof(int),
-                                cudaMemcpyDeviceToHost, b->stream));
-            BCK(cudaEventRecord(b->polled[slot], b->stream));
-            if (polls > 0) {
-                BCK(cudaEventSynchronize(b->polled[1 - slot]));
-                if (b->h_nactive[1 - slot] == 0) all_done = true;
-            }
-            polls++;
-        }
-        s = e;
-    }
-    BCK(cudaEventRecord(b->ev1, b->stream));
-    k_batch_gather<<<(n + 127) / 128, 128, 0, b->stream>>>(b->checks, n, b->outs);
-    BCK(cudaGetLastError());
-    BCK(cudaMemcpyAsync(b->h_outs, b->outs, n * sizeof(BatchOut), cudaMemcpyDeviceToHost,
-                        b->stream));
-    BCK(cudaStreamSynchronize(b->stream));
-    float ms = 0.f;
-    BCK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
-    bool any_check = false;
-    for (const SegSpec& sg : sched)
-        if (sg.i1 <= steps_run) any_check |= sg.check;
-    double point_steps = 0;
-    for (int i = 0; i < n; ++i) {
-        gpue_ctx* c = b->ctx[i];
-        const BatchOut& bo = b->h_outs[i];
-        const bool stopped = bo.active == 0;
-        const int steps = stopped ? bo.steps : steps_run;
-        point_steps += (double)c->N * steps;
-        if (results) {
-            results[i].steps_done = steps;
-            results[i].early_stop = stopped ? 1 : 0;
-            results[i].energy = any_check ? bo.energy : NAN;
-        }
-        if (any_check) c->last_energy = bo.energy;
-        if (gstate == 0) c->pending_scale = true;
-        BCTX(c, apply_pending_scale(c, c->prec));
-        bool guard = false;
-        for (const BGroup& g : r.groups)
-            for (int m : g.members)
-                if (m == i) guard = g.guard;
-        if (guard) BCTX(c, scale_state(c, c->prec, kGuard));
-    }
-    for (int i = 0; i < n; ++i) BCK(cudaStreamSynchronize(b->ctx[i]->stream));
-    if (stats) {
-        stats->device_ms = ms;
-        stats->kernel_launches = launches;
-        stats->graph_launches = glaunches;
-        stats->point_steps = point_steps;
     }
     return GPUE_OK;
 }

@@ -230,6 +230,72 @@ const char* gpue_batch_last_error(const gpue_batch* batch);
 gpue_status gpue_batch_evolve(gpue_batch* batch, int32_t gstate, const gpue_batch_opts* opts,
                               gpue_batch_result* results, gpue_batch_stats* stats);
 
+/* ---- serving (no counterpart in GPUE): a request loop on one device that
+ * admits solves as HBM budget and slots free up, keeps each admitted solve's
+ * wavefunction and operators resident, and steps all resident solves together
+ * (continuous batching).  A worker thread runs ticks of check_steps steps:
+ * every tick advances every resident solve by check_steps steps (solves of
+ * one kind share launches as in gpue_batch_*), then checks each one's energy;
+ * a solve leaves at the tick where it meets the threshold (imaginary time) or
+ * reaches max_steps, and requests that arrived meanwhile are admitted before
+ * the next tick.  A solve's arithmetic does not depend on the other solves
+ * resident with it: its result is the same alone and in any mix. */
+typedef struct gpue_server gpue_server;
+
+typedef struct gpue_server_opts {
+    int32_t device;
+    int32_t precision;         /* form of every solve: GPUE_PREC_FP32 or GPUE_PREC_FP64 */
+    int64_t hbm_budget_bytes;  /* device bytes resident solves may hold; 0: 90% of free */
+    int32_t check_steps;       /* steps per tick and between energy checks (even, >= 2) */
+    int32_t max_active;        /* resident solves at most; 0: no limit */
+    double threshold;          /* imaginary-time stop between consecutive checks */
+    int32_t threshold_abs;     /* 1: |E_old-E| < threshold; 0: |E_old-E| < threshold*E_old */
+    int32_t reserved[7];
+} gpue_server_opts;
+
+typedef struct gpue_request {
+    gpue_params params;  /* grid and physics; precision and device are the server's */
+    int32_t gstate;      /* 0: imaginary time until the threshold, 1: real time */
+    int32_t max_steps;   /* a multiple of check_steps */
+    const void* psi0;    /* host complex128, read when the solve is admitted */
+    void* psi_out;       /* host complex128, written when it completes; may be NULL */
+    int64_t tag;         /* returned with the result */
+} gpue_request;
+
+typedef struct gpue_server_result {
+    int64_t tag;
+    int32_t status;      /* gpue_status of this solve */
+    int32_t steps_done;
+    int32_t early_stop;
+    int32_t reserved0;
+    double energy;       /* energy at the last check */
+    double t_submit, t_admit, t_done;  /* seconds on the server clock */
+} gpue_server_result;
+
+typedef struct gpue_server_stats {
+    int64_t submitted, admitted, completed, failed;
+    int32_t active, queued;
+    int64_t bytes_resident, bytes_peak, bytes_budget;
+    int64_t ticks, kernel_launches;
+    double point_steps;  /* grid points x steps run by all ticks */
+    double busy_s;       /* device time of the ticks (CUDA events) */
+} gpue_server_stats;
+
+gpue_status gpue_server_create(const gpue_server_opts* opts, gpue_server** out);
+/* Stops the worker; queued and resident solves are dropped. */
+gpue_status gpue_server_destroy(gpue_server* server);
+const char* gpue_server_last_error(const gpue_server* server);
+/* Queues a request (thread-safe); psi0 and psi_out must stay valid until its
+ * result is polled. */
+gpue_status gpue_server_submit(gpue_server* server, const gpue_request* req);
+/* Moves up to cap finished results into out (*n of them), waiting up to
+ * timeout_s seconds when none is ready. */
+gpue_status gpue_server_poll(gpue_server* server, gpue_server_result* out, int32_t cap,
+                             int32_t* n, double timeout_s);
+gpue_status gpue_server_get_stats(gpue_server* server, gpue_server_stats* stats);
+/* Seconds since the server was created (the clock of the result times). */
+double gpue_server_clock(const gpue_server* server);
+
 #ifdef __cplusplus
 }
 #endif

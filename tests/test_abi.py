@@ -72,3 +72,20 @@ def test_invalid_arguments_fail_without_touching_the_device():
     assert L.gpue_batch_evolve(None, 0, None, None, None) == 1
     assert L.gpue_batch_destroy(None) == 0
     assert L.gpue_batch_last_error(None) == b""
+
+
+def test_server_arguments_fail_without_touching_the_device():
+    import gpue_b200 as G
+    L = G.lib()
+    h = ctypes.c_void_p()
+    o = G.ServerOpts()
+    o.precision, o.check_steps = G.PREC_FP32, 3  # odd tick lengths are rejected
+    assert L.gpue_server_create(ctypes.byref(o), ctypes.byref(h)) == 1
+    o.check_steps, o.precision = 100, 7
+    assert L.gpue_server_create(ctypes.byref(o), ctypes.byref(h)) == 1
+    assert L.gpue_server_create(None, ctypes.byref(h)) == 1
+    assert L.gpue_server_submit(None, None) == 1
+    n = ctypes.c_int32()
+    assert L.gpue_server_poll(None, None, 0, ctypes.byref(n), 0.0) == 1
+    assert L.gpue_server_destroy(None) == 0
+    assert L.gpue_server_last_error(None) == b""
