@@ -53,6 +53,8 @@ def parse_args():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="skip the steady-state and e2e legs")
+    ap.add_argument("--only", choices=["batch", "serve"], default=None,
+                    help="run one auxiliary leg alone and print its JSON")
     ap.add_argument("--profile", choices=["fp32", "fp64"], default=None,
                     help="profiling case for ncu: the same workload without the relaxation "
                          "prep, --warmup + --steps time steps of one form, no timing output")
@@ -235,6 +237,188 @@ def accuracy_leg(G, psi0, dev, nsteps=2000):
             "dE_rel": abs(out["fp32"] - out["fp64"]) / abs(out["fp64"])}
 
 
+# ------------------------------------------------- batched sweep ----------
+
+# 96 independent 2D ground-state solves (seed 4): n ~ U{128,192,256,384,512},
+# g ~ U[10,1000], wy/wx ~ U[0.8,1.25], box [-10,10)^2, dt = 1e-4, checks
+# every 100 steps with the absolute |dE| < 1e-10 stop, fused complex64.
+BATCH = dict(solves=96, sizes=(128, 192, 256, 384, 512), box=10.0, gdt=1e-4, every=100,
+             thr=1e-10, seed=4)
+# the sample timed: steps 0..1000 (checks at 0, 100, ..., 1000) of every solve
+BATCH_STEPS = 1001
+
+
+def gauss_start(dim, n, box, seed):
+    """exp(-r^2/2) (1 + 0.01 xi), xi ~ N(0,1) iid (PCG64 seed), complex128."""
+    import numpy as np
+    dx = box / (n >> 1)
+    x = -box + dx * np.arange(n)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    if dim == 2:
+        r2 = x[None, :] ** 2 + x[:, None] ** 2
+    else:
+        r2 = x[None, None, :] ** 2 + x[None, :, None] ** 2 + x[:, None, None] ** 2
+    psi = np.exp(-r2 / 2.0) * (1.0 + 0.01 * rng.standard_normal(r2.shape))
+    return psi.astype(np.complex128)
+
+
+def batch_cases():
+    import numpy as np
+    rng = np.random.Generator(np.random.PCG64(BATCH["seed"]))
+    out = []
+    for k in range(BATCH["solves"]):
+        n = int(rng.choice(BATCH["sizes"]))
+        g = float(rng.uniform(10.0, 1000.0))
+        wy = float(rng.uniform(0.8, 1.25))
+        out.append(dict(n=n, g=g, wy=wy, seed=1000 + k))
+    return out
+
+
+def batch_leg(G, dev, steps=BATCH_STEPS):
+    """The 96 solves as one gpue_batch against the same solves run one after
+    another through gpue_evolve (same form, same checks)."""
+    cs = batch_cases()
+    psi0 = [gauss_start(2, c["n"], BATCH["box"], c["seed"]) for c in cs]
+
+    def params(c):
+        return G.make_params(2, c["n"], BATCH["box"], wy=c["wy"], g=c["g"], gdt=BATCH["gdt"],
+                             precision=G.PREC_FP32, device=dev)
+
+    kw = dict(energy_every=BATCH["every"], threshold=BATCH["thr"], threshold_abs=True)
+    solvers = [G.Solver(params(c)) for c in cs]
+    try:
+        for s, p in zip(solvers, psi0):
+            s.set_wfc(p)
+        with G.Batch(solvers) as b:
+            b.evolve(0, 2 * BATCH["every"] + 1, **kw)  # captures the graphs
+            for s, p in zip(solvers, psi0):
+                s.set_wfc(p)
+            res, st = b.evolve(0, steps, **kw)
+        batched = st["point_steps"] / (st["device_ms"] * 1e-3)
+        # sequential: the same solves, one gpue_evolve call each
+        seq_ms, seq_pts = 0.0, 0.0
+        for s, p, c in zip(solvers, psi0, cs):
+            s.set_wfc(p)
+            s.evolve(2 * BATCH["every"] + 1, 0, **kw)  # graphs of this solve
+            s.set_wfc(p)
+            r = s.evolve(steps, 0, **kw)
+            seq_ms += r["device_ms"]
+            seq_pts += c["n"] ** 2 * r["steps_done"]
+    finally:
+        for s in solvers:
+            s.close()
+    return {"solves": len(cs), "steps": steps, "value": batched, "unit": UNIT,
+            "device_ms": st["device_ms"], "kernel_launches": st["kernel_launches"],
+            "graph_launches": st["graph_launches"],
+            "stopped": sum(r["early_stop"] for r in res),
+            "sequential_value": seq_pts / (seq_ms * 1e-3), "sequential_device_ms": seq_ms,
+            "batched_over_sequential": batched / (seq_pts / (seq_ms * 1e-3)),
+            "sample": "steps 0..%d of all 96 solves (checks every 100 steps, |dE|<1e-10 "
+                      "absolute stop; none is expected to stop this early), complex64 with "
+                      "FP64 reductions; sequential = the same solves through gpue_evolve one "
+                      "after another (sum of their device times)" % (steps - 1)}
+
+
+# -------------------------------------------------------------- serving ---
+
+# Poisson arrivals at 200/s (seed 5): 70% 2D with n ~ U{128..1024}, 30% 3D
+# with n ~ U{64..192}, each rounded up to the next compiled FFT length; half
+# imaginary time (|dE| < 1e-10 between 100-step checks), half real time for
+# 2000 steps with Omega ~ U[0, 0.8]; g ~ U[10, 1000]; 150 GB HBM budget.
+SERVE = dict(rate=200.0, seed=5, budget=150e9, check=100, thr=1e-10, real_steps=2000,
+             imag_cap=2000, requests=40)
+
+
+def round_up_length(G, n, precision):
+    m = n
+    while not G.supported_length(m, precision):
+        m += 1
+    return m
+
+
+def serve_requests(G):
+    import numpy as np
+    rng = np.random.Generator(np.random.PCG64(SERVE["seed"]))
+    t, out = 0.0, []
+    for k in range(SERVE["requests"]):
+        t += float(rng.exponential(1.0 / SERVE["rate"]))
+        dim = 2 if rng.random() < 0.7 else 3
+        n = int(rng.integers(128, 1025)) if dim == 2 else int(rng.integers(64, 193))
+        n = round_up_length(G, n, G.PREC_FP32)
+        gs = 0 if rng.random() < 0.5 else 1
+        omega = float(rng.uniform(0.0, 0.8)) if gs == 1 else 0.0
+        g = float(rng.uniform(10.0, 1000.0))
+        out.append(dict(t=t, dim=dim, n=n, gstate=gs, omega=omega, g=g, seed=5000 + k,
+                        box=10.0 if dim == 2 else 8.0,
+                        steps=SERVE["real_steps"] if gs == 1 else SERVE["imag_cap"]))
+    return out
+
+
+def serve_params(G, q, precision, dev):
+    return G.make_params(q["dim"], q["n"], q["box"], g=q["g"], omega=q["omega"],
+                         gauge=q["omega"] != 0.0, gdt=1e-4, dt=5e-5, precision=precision,
+                         device=dev)
+
+
+def serve_leg(G, dev):
+    """The request stream through gpue_server (fused complex64, continuous
+    batching) against the same requests as sequential plain FP64 solves."""
+    import threading
+    import numpy as np
+    reqs = serve_requests(G)
+    psi0 = [gauss_start(q["dim"], q["n"], q["box"], q["seed"]) for q in reqs]
+    results = {}
+    with G.Server(precision=G.PREC_FP32, check_steps=SERVE["check"], threshold=SERVE["thr"],
+                  threshold_abs=True, hbm_budget=SERVE["budget"], device=dev) as srv:
+        t0 = time.perf_counter()
+
+        def submitter():
+            for k, q in enumerate(reqs):
+                delay = q["t"] - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+                srv.submit(serve_params(G, q, G.PREC_FP32, dev), q["gstate"], q["steps"],
+                           psi0[k], k)
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        deadline = time.perf_counter() + 600
+        while len(results) < len(reqs) and time.perf_counter() < deadline:
+            for r in srv.poll(timeout=0.5):
+                results[r["tag"]] = r
+        th.join()
+        wall = time.perf_counter() - t0
+        stats = srv.stats()
+    lat = np.array([r["t_done"] - r["t_submit"] for r in results.values()])
+    ok = sum(1 for r in results.values() if r["status"] == 0)
+    # sequential plain FP64, one gpue_evolve per request, host buffers in and out
+    t1 = time.perf_counter()
+    for k, q in enumerate(reqs):
+        with G.Solver(serve_params(G, q, G.PREC_FP64, dev)) as s:
+            s.set_wfc(psi0[k])
+            if q["gstate"] == 0:
+                s.evolve(q["steps"], 0, energy_every=SERVE["check"], threshold=SERVE["thr"],
+                         threshold_abs=True)
+            else:
+                s.evolve(q["steps"], 1)
+            s.get_wfc()
+    seq_wall = time.perf_counter() - t1
+    return {"requests": len(reqs), "completed": ok, "wall_s": wall,
+            "solves_per_s": ok / wall, "latency_p50_s": float(np.percentile(lat, 50)),
+            "latency_p99_s": float(np.percentile(lat, 99)),
+            "sequential_plain_fp64_solves_per_s": len(reqs) / seq_wall,
+            "sequential_wall_s": seq_wall,
+            "served_over_sequential": (ok / wall) / (len(reqs) / seq_wall),
+            "device_busy_s": stats["busy_s"], "ticks": stats["ticks"],
+            "kernel_launches": stats["kernel_launches"],
+            "point_steps_per_s": stats["point_steps"] / wall,
+            "bytes_peak": stats["bytes_peak"],
+            "sample": "the first %d requests of the seeded stream (arrivals over %.2f s); "
+                      "imaginary-time solves capped at %d steps; wall-clock from the first "
+                      "arrival to the last result, results copied to host buffers"
+                      % (len(reqs), reqs[-1]["t"], SERVE["imag_cap"])}
+
+
 # ------------------------------------------------------------- CPU --------
 
 def cpu_oracle_rate(psi0, budget_s=12.0, threads=0):
@@ -331,6 +515,10 @@ def main():
         return
     import torch
     import gpue_b200 as G
+    if args.only:
+        leg = batch_leg if args.only == "batch" else serve_leg
+        print(json.dumps({args.only: leg(G, 0)}), flush=True)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -406,6 +594,8 @@ def main():
         cpu = cpu_oracle_rate(psi0)
     e2e = None if args.quick else e2e_leg(G, torch, psi0, dev)
     acc = accuracy_leg(G, psi0, dev)
+    batched = None if args.quick else batch_leg(G, dev)
+    served = None if args.quick else serve_leg(G, dev)
     line = {
         "metric": METRIC, "value": v32, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": res["fp32"]["ms"] / args.steps,
@@ -423,6 +613,7 @@ def main():
                          "note": "one gpue_evolve call of 20000 steps (the configuration's "
                                  "length), graph-replayed, no L2 flush"},
         "accuracy": acc,
+        "batched_sweep": batched, "serving": served,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
         "clocks": res["fp32"]["clocks"],
         "gpu_launches": res["fp32"]["launches"],
