@@ -142,9 +142,11 @@ gpue_status plan_segment(const BatchRun& r, int s0, int s1, bool check, ArgSink&
             const unsigned grid = (unsigned)(n * lc.ntiles);
             const unsigned threads = (unsigned)lc.threads;
             const size_t smem = lc.smem;
+            const bool pdl = j > 0;  // follows a pass kernel on this lane
             sp.lanes[gi].push_back([=](cudaStream_t s) {
-                fn<<<grid, threads, smem, s>>>(static_cast<const PassArgs*>(dargs),
-                                               static_cast<const long*>(dprefix), n);
+                launch_kernel(fn, grid, threads, smem, s, pdl,
+                              static_cast<const PassArgs*>(dargs),
+                              static_cast<const long*>(dprefix), n);
             });
             sp.launches++;
         }

@@ -210,7 +210,7 @@ gpue_status plan_axis(gpue_ctx* c, int prec, int axis) {
         const int min_c = (32 + k->elem - 1) / k->elem;  // one 32-byte sector per row
         C = 128 / k->p;
         if (C < min_c) C = min_c;
-        if (C * k->p > kMaxPassThreads) C = kMaxPassThreads / k->p;
+        if (C * k->p > k->max_threads) C = k->max_threads / k->p;
         while (C > 1 && c->ax[0].n % C) C >>= 1;
     }
     while (C > 1 && nlines % C) C >>= 1;
@@ -302,7 +302,8 @@ gpue_status make_pass_args(gpue_ctx* c, int prec, const LPass& lp, int gstate, P
     return GPUE_OK;
 }
 
-gpue_status launch_pass(gpue_ctx* c, int prec, const LPass& lp, int gstate) {
+// pdl: the previous operation in the stream is a pass kernel
+gpue_status launch_pass(gpue_ctx* c, int prec, const LPass& lp, int gstate, bool pdl) {
     PassArgs a;
     gpue_status st = make_pass_args(c, prec, lp, gstate, a);
     if (st) return st;
@@ -310,9 +311,8 @@ gpue_status launch_pass(gpue_ctx* c, int prec, const LPass& lp, int gstate) {
     const LaunchCfg& lc = c->lc[prec][lp.axis];
     void (*fn)(PassArgs) = lp.axis == 0 ? (c->ext ? lc.k->row_ext : lc.k->row)
                                         : (c->ext ? lc.k->col_ext : lc.k->col);
-    fn<<<lc.blocks, lc.threads, lc.smem, c->stream>>>(a);
+    CK(launch_kernel(fn, lc.blocks, lc.threads, lc.smem, c->stream, pdl, a));
     c->launches++;
-    CK(cudaGetLastError());
     return GPUE_OK;
 }
 
@@ -473,10 +473,14 @@ EnergyArgs energy_args(gpue_ctx* c, int prec, bool scale_pending) {
     return e;
 }
 
-gpue_status launch_energy(gpue_ctx* c, int prec, int gstate, bool scale_pending) {
+// after_pass: the energy passes follow a pass kernel in the stream
+gpue_status launch_energy(gpue_ctx* c, int prec, int gstate, bool scale_pending,
+                          bool after_pass = false) {
+    bool pdl = after_pass;
     for (auto& lp : energy_passes(c, scale_pending)) {
-        gpue_status st = launch_pass(c, prec, lp, gstate);
+        gpue_status st = launch_pass(c, prec, lp, gstate, pdl);
         if (st) return st;
+        pdl = true;
     }
     EnergyArgs e = energy_args(c, prec, scale_pending);
     const int blocks = c->sms * 4;
@@ -550,12 +554,12 @@ gpue_status enqueue_steps(gpue_ctx* c, int prec, int i0, int i1, int gstate, boo
         step_passes(c, i, gstate, i == i0 ? scale_first : gstate == 0,
                     rexp.empty() ? 1.0 : rexp[i], guard, v);
     if (!c->time_dep) fuse(v);  // fused passes would mix two steps' times
-    for (auto& lp : v) {
-        gpue_status st = launch_pass(c, prec, lp, gstate);
+    for (size_t k = 0; k < v.size(); ++k) {
+        gpue_status st = launch_pass(c, prec, v[k], gstate, k > 0);
         if (st) return st;
     }
     if (energy_after) {
-        gpue_status st = launch_energy(c, prec, gstate, gstate == 0);
+        gpue_status st = launch_energy(c, prec, gstate, gstate == 0, !v.empty());
         if (st) return st;
     }
     return GPUE_OK;

@@ -159,6 +159,25 @@ struct LPass {
     double time = 0;           // Dt * step, for time-dependent expressions
 };
 
+// Launches a kernel; with `pdl` it may start while the previous kernel in the
+// stream is finishing (programmatic dependent launch): only for pass kernels
+// that follow a pass kernel, which wait for their predecessor (pdl_wait).
+template <typename... P, typename... A>
+inline cudaError_t launch_kernel(void (*fn)(P...), unsigned grid, unsigned threads, size_t smem,
+                                 cudaStream_t s, bool pdl, A&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = pdl ? at : nullptr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, fn, std::forward<A>(args)...);
+}
+
 size_t elem_size(int prec);
 int kprec(int prec);
 void* state_of(gpue_ctx* c, int prec);

@@ -196,23 +196,29 @@ struct SmallDFT {
 
 __host__ __device__ __forceinline__ constexpr int smem_phys(int i) { return i + (i >> 4); }
 
-template <typename T, int N_, int RA, int RB, int P_>
+template <typename T, int N_, int RA, int RB, int P_, int RC = 0>
 struct LineFFT {
     static constexpr int N = N_;
     static constexpr int P = P_;
-    static constexpr int NS = RB ? 3 : 2;
+    static constexpr int NS = RB == 0 ? 2 : RC == 0 ? 3 : 4;
     static constexpr int E = N / P;
-    static_assert(NS == 2 ? N == RA * RA : N == RA * RB * RA, "palindromic radix plan");
+    static_assert(NS == 2   ? N == RA * RA
+                  : NS == 3 ? N == RA * RB * RA
+                            : N == RA * RB * RC * RA,
+                  "palindromic radix plan");
     static_assert((N / RA) % P == 0, "threads must divide the butterflies of the outer stages");
-    static_assert(NS == 2 || (N / RB) % P == 0, "threads must divide the middle stage");
+    static_assert(NS == 2 || (N / RB) % P == 0, "threads must divide the middle stages");
+    static_assert(NS < 4 || (N / RC) % P == 0, "threads must divide the middle stages");
     // smem line stride in complex elements: one pad per 16, rounded to 16 and
     // offset by 4 so the lines a strided-pass warp touches (lanes c + C*t)
     // fall on distinct banks
     static constexpr int LS = ((smem_phys(N - 1) + 1 + 15) / 16) * 16 + 4;
 
-    __host__ __device__ static constexpr int radix(int s) { return (NS == 3 && s == 1) ? RB : RA; }
+    __host__ __device__ static constexpr int radix(int s) {
+        return s == 0 || s == NS - 1 ? RA : s == 1 ? RB : RC;
+    }
     __host__ __device__ static constexpr int ns_before(int s) {
-        return s == 0 ? 1 : s == 1 ? RA : RA * RB;
+        return s == 0 ? 1 : s == 1 ? RA : s == 2 ? RA * RB : RA * RB * RC;
     }
 
     // element index held by register e in layout D
@@ -220,20 +226,54 @@ struct LineFFT {
         return t + P * (e / RA) + (e % RA) * (N / RA);
     }
 
+    // The twiddles stage S > 0 multiplies by.  When few enough, they are
+    // loaded into registers before the exchange that precedes the stage, so
+    // their latency overlaps the shared-memory round trip; when P is a
+    // multiple of Ns they depend on t only and one set serves every group.
+    // Larger sets (long odd-radix plans) are read at use, as registers are
+    // scarce there.
     template <int S>
-    static __device__ __forceinline__ void compute(cx<T> (&v)[E], int t,
-                                                   const cx<T>* __restrict__ tw) {
+    struct StageTw {
+        static constexpr int R = radix(S);
+        static constexpr int Ns = ns_before(S);
+        static constexpr int G = N / (R * P);
+        static constexpr int step = N / (Ns * R);
+        static constexpr int NQ = (S > 0 && P % Ns == 0) ? 1 : G;
+        static constexpr bool HOLD = NQ * (R - 1) <= 16;
+        cx<T> w[HOLD ? NQ : 1][HOLD ? R - 1 : 1];
+        const cx<T>* __restrict__ tw;
+        int t;
+
+        __device__ __forceinline__ void load(int t_, const cx<T>* __restrict__ tw_) {
+            t = t_;
+            tw = tw_;
+            if constexpr (HOLD) {
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) {
+                    const int jm = (t + P * q) % Ns;
+#pragma unroll
+                    for (int r = 1; r < R; ++r) w[q][r - 1] = tw[jm * r * step];
+                }
+            }
+        }
+        __device__ __forceinline__ cx<T> get(int q, int r) const {
+            if constexpr (HOLD) {
+                return w[NQ == 1 ? 0 : q][r - 1];
+            } else {
+                return tw[((t + P * q) % Ns) * r * step];
+            }
+        }
+    };
+
+    template <int S>
+    static __device__ __forceinline__ void compute(cx<T> (&v)[E], const StageTw<S>* w) {
         constexpr int R = radix(S);
-        constexpr int Ns = ns_before(S);
         constexpr int G = N / (R * P);
 #pragma unroll
         for (int q = 0; q < G; ++q) {
             if constexpr (S > 0) {
-                const int j = t + P * q;
-                const int jm = j % Ns;
-                constexpr int step = N / (Ns * R);
 #pragma unroll
-                for (int r = 1; r < R; ++r) v[q * R + r] = cmul(v[q * R + r], tw[jm * r * step]);
+                for (int r = 1; r < R; ++r) v[q * R + r] = cmul(v[q * R + r], w->get(q, r));
             }
             SmallDFT<R, T>::run(&v[q * R]);
         }
@@ -264,17 +304,25 @@ struct LineFFT {
         sync();
     }
 
+    // One stage after the first: its twiddles are requested before the
+    // exchange, so their latency overlaps the shared-memory round trip.
+    template <int S, typename Sync>
+    static __device__ __forceinline__ void stage(cx<T> (&v)[E], int t, cx<T>* sl,
+                                                 const cx<T>* __restrict__ tw, Sync sync) {
+        StageTw<S> w;
+        w.load(t, tw);
+        exchange<S - 1>(v, t, sl, sync);
+        compute<S>(v, &w);
+    }
+
     // Unnormalised forward DFT of the line (inverse: conjugate around it).
     template <typename Sync>
     static __device__ __forceinline__ void forward(cx<T> (&v)[E], int t, cx<T>* sl,
                                                    const cx<T>* __restrict__ tw, Sync sync) {
-        compute<0>(v, t, tw);
-        exchange<0>(v, t, sl, sync);
-        compute<1>(v, t, tw);
-        if constexpr (NS == 3) {
-            exchange<1>(v, t, sl, sync);
-            compute<2>(v, t, tw);
-        }
+        compute<0>(v, static_cast<const StageTw<0>*>(nullptr));
+        stage<1>(v, t, sl, tw, sync);
+        if constexpr (NS >= 3) stage<2>(v, t, sl, tw, sync);
+        if constexpr (NS >= 4) stage<3>(v, t, sl, tw, sync);
     }
 };
 

@@ -209,42 +209,48 @@ __device__ __forceinline__ cx<T> apply(cx<T> v, cx<double> f) {
     }
 }
 
-// exp(-i a) for 0 <= a < 1/16 by its Taylor series (truncation error below
-// a^9/9! < 4e-17), else by sincos; |result| = 1 to FP64 accuracy.
 template <typename T>
 __device__ __forceinline__ cx<double> unit_phase(double a);
 
+// exp(-i a) for |a| < 1/16 by its Taylor series (truncation error below
+// a^9/9! < 4e-17, so |result| = 1 to FP64 accuracy), no branch
+__device__ __forceinline__ cx<double> taylor_phase(double a) {
+    const double a2 = a * a;
+    const double s = a * (1.0 - a2 * (1.0 / 6.0 - a2 * (1.0 / 120.0 - a2 * (1.0 / 5040.0))));
+    const double c =
+        1.0 - a2 * (0.5 - a2 * (1.0 / 24.0 - a2 * (1.0 / 720.0 - a2 * (1.0 / 40320.0))));
+    return {c, -s};
+}
+
+// exp(-i a): the Taylor series for |a| < 1/16, else sincos
 template <typename T>
 __device__ __forceinline__ cx<double> small_phase(double a) {
-    if (fabs(a) < 0.0625) {
-        const double a2 = a * a;
-        const double s = a * (1.0 - a2 * (1.0 / 6.0 - a2 * (1.0 / 120.0 - a2 * (1.0 / 5040.0))));
-        const double c =
-            1.0 - a2 * (0.5 - a2 * (1.0 / 24.0 - a2 * (1.0 / 720.0 - a2 * (1.0 / 40320.0))));
-        return {c, -s};
-    }
+    if (fabs(a) < 0.0625) return taylor_phase(a);
     return unit_phase<T>(a);
 }
 
-// exp(-a) for 0 <= a < 1/16 by its Taylor series (truncation error below
-// a^10/10! < 5e-19), else by exp.
 template <typename T>
 __device__ __forceinline__ double decay(double a);
 
+// exp(-a) for |a| < 1/16 by its Taylor series (truncation error below
+// a^10/10! < 5e-19), no branch
+__device__ __forceinline__ double taylor_decay(double a) {
+    double r = 1.0 / 362880.0;
+    r = 1.0 / 40320.0 - a * r;
+    r = 1.0 / 5040.0 - a * r;
+    r = 1.0 / 720.0 - a * r;
+    r = 1.0 / 120.0 - a * r;
+    r = 1.0 / 24.0 - a * r;
+    r = 1.0 / 6.0 - a * r;
+    r = 0.5 - a * r;
+    r = 1.0 - a * r;
+    return 1.0 - a * r;
+}
+
+// exp(-a): the Taylor series for |a| < 1/16, else exp
 template <typename T>
 __device__ __forceinline__ double small_decay(double a) {
-    if (fabs(a) < 0.0625) {
-        double r = 1.0 / 362880.0;
-        r = 1.0 / 40320.0 - a * r;
-        r = 1.0 / 5040.0 - a * r;
-        r = 1.0 / 720.0 - a * r;
-        r = 1.0 / 120.0 - a * r;
-        r = 1.0 / 24.0 - a * r;
-        r = 1.0 / 6.0 - a * r;
-        r = 0.5 - a * r;
-        r = 1.0 - a * r;
-        return 1.0 - a * r;
-    }
+    if (fabs(a) < 0.0625) return taylor_decay(a);
     return decay<T>(a);
 }
 
@@ -274,6 +280,18 @@ __device__ __forceinline__ double decay(double a) {
 
 constexpr int kMaxPassThreads = 256;
 
+// Programmatic dependent launch: once a pass kernel's CTAs have finished
+// their tiles, the next pass kernel in the stream may start launching (its
+// CTAs become resident while this grid drains), and every pass kernel waits
+// for the grid before it to complete -- with its memory visible -- before
+// touching any data.  Both are no-ops for a kernel launched without the
+// programmatic-serialization attribute.
+__device__ __forceinline__ void pdl_launch_dependents() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+
 // C = blockDim.x / P lines per tile; CTAs walk tiles with a grid stride.
 // make_complex (src/kernels.cu:165-187): 1 -> exp(-v), 2 -> exp(-i v)
 __device__ __forceinline__ cx<double> make_complex_ev(double v, int type) {
@@ -286,10 +304,10 @@ __device__ __forceinline__ cx<double> make_complex_ev(double v, int type) {
 // EXT: also the table and expression forms of the factor ops.
 // Tiles t0, t0 + tstep, ... of one field; returns this thread's OP_NORM /
 // OP_EKIN accumulation.
-template <typename T, int N, int RA, int RB, int P, bool STRIDED, bool EXT>
+template <typename T, int N, int RA, int RB, int P, bool STRIDED, bool EXT, int RC = 0>
 __device__ __forceinline__ KSum pass_tiles(const PassArgs& a, long t0, long tstep,
                                            unsigned char* smem_raw) {
-    using L = LineFFT<T, N, RA, RB, P>;
+    using L = LineFFT<T, N, RA, RB, P, RC>;
     constexpr int E = L::E;
 
     const int C = blockDim.x / P;
@@ -404,16 +422,51 @@ __device__ __forceinline__ KSum pass_tiles(const PassArgs& a, long t0, long tste
                     else if (a.axis == 1) lf = cmul(ld2(a.vfac[0], xi), ld2(a.vfac[2], zi));
                     else lf = cmul(ld2(a.vfac[0], xi), ld2(a.vfac[1], yi));
                     const double2* fa = a.vfac[a.axis];
+                    // The nonlinear angle gN|psi|^2 Dt/(2 hbar) is almost always
+                    // below 1/16, where a Taylor series is exact to FP64: decide
+                    // that once for the thread's values (an FP32 estimate with
+                    // margin), so the unrolled loop below has no branch and the
+                    // values' FP64 chains interleave.
+                    bool small = true;
+                    if (a.gpe) {
+                        const float nl = (float)a.nl_coef;
+                        float m = 0.f;
 #pragma unroll
-                    for (int e = 0; e < E; ++e) {
-                        cx<double> f = cmul(ld2(fa, L::index(t, e)), lf);
-                        if (a.gpe) {
+                        for (int e = 0; e < E; ++e)
+                            m = fmaxf(m, fabsf(nl * ((float)v[e].x * (float)v[e].x +
+                                                     (float)v[e].y * (float)v[e].y)));
+                        small = m < 0.06f;
+                    }
+                    if (!a.gpe) {
+#pragma unroll
+                        for (int e = 0; e < E; ++e)
+                            v[e] = apply(v[e], cmul(ld2(fa, L::index(t, e)), lf));
+                    } else if (small && a.gstate == 0) {
+#pragma unroll
+                        for (int e = 0; e < E; ++e) {
+                            const double gd = a.nl_coef * ((double)v[e].x * v[e].x +
+                                                           (double)v[e].y * v[e].y);
+                            const cx<double> f = cmul(ld2(fa, L::index(t, e)), lf);
+                            v[e] = apply(v[e], cscale(f, taylor_decay(gd)));
+                        }
+                    } else if (small) {
+#pragma unroll
+                        for (int e = 0; e < E; ++e) {
+                            const double gd = a.nl_coef * ((double)v[e].x * v[e].x +
+                                                           (double)v[e].y * v[e].y);
+                            const cx<double> f = cmul(ld2(fa, L::index(t, e)), lf);
+                            v[e] = apply(v[e], cmul(f, taylor_phase(gd)));
+                        }
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < E; ++e) {
+                            cx<double> f = cmul(ld2(fa, L::index(t, e)), lf);
                             const double gd = a.nl_coef * ((double)v[e].x * v[e].x +
                                                            (double)v[e].y * v[e].y);
                             if (a.gstate == 0) f = cscale(f, small_decay<T>(gd));
                             else f = cmul(f, small_phase<T>(gd));
+                            v[e] = apply(v[e], f);
                         }
-                        v[e] = apply(v[e], f);
                     }
                     break;
                 }
@@ -561,10 +614,17 @@ __device__ __forceinline__ KSum pass_tiles(const PassArgs& a, long t0, long tste
 }
 
 // One field: a persistent grid walks the tiles.
-template <typename T, int N, int RA, int RB, int P, bool STRIDED, bool EXT>
-__global__ void __launch_bounds__(kMaxPassThreads, 2) k_pass(const PassArgs a) {
+// MAXT threads per CTA at most, MINB resident CTAs per SM: the register
+// budget per thread is 65536 / (MAXT * MINB) (256 x 2: 128 registers;
+// 512 x 2: 64 registers for plans with 8 values per thread).
+template <typename T, int N, int RA, int RB, int P, bool STRIDED, bool EXT, int RC = 0,
+          int MAXT = kMaxPassThreads, int MINB = 2>
+__global__ void __launch_bounds__(MAXT, MINB) k_pass(const PassArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    KSum acc = pass_tiles<T, N, RA, RB, P, STRIDED, EXT>(a, blockIdx.x, gridDim.x, smem_raw);
+    pdl_wait();
+    KSum acc =
+        pass_tiles<T, N, RA, RB, P, STRIDED, EXT, RC>(a, blockIdx.x, gridDim.x, smem_raw);
+    pdl_launch_dependents();
     if (a.red.kind != RED_NONE) {
         __syncthreads();  // smem is reused as reduction scratch
         grid_reduce_finish(acc, reinterpret_cast<double*>(smem_raw), a.red, gridDim.x,
@@ -575,11 +635,13 @@ __global__ void __launch_bounds__(kMaxPassThreads, 2) k_pass(const PassArgs a) {
 // Many fields of the same length at once (independent solves): one CTA per
 // tile, tile_prefix[s] the first CTA of solve s.  A solve whose *active flag
 // is 0 (converged) is skipped; each solve reduces over its own tiles.
-template <typename T, int N, int RA, int RB, int P, bool STRIDED>
-__global__ void __launch_bounds__(kMaxPassThreads, 2)
+template <typename T, int N, int RA, int RB, int P, bool STRIDED, int RC = 0,
+          int MAXT = kMaxPassThreads, int MINB = 2>
+__global__ void __launch_bounds__(MAXT, MINB)
     k_pass_batch(const PassArgs* __restrict__ args, const long* __restrict__ tile_prefix,
                  int nsolves) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    pdl_wait();
     const long b = blockIdx.x;
     int lo = 0, hi = nsolves - 1;
     while (lo < hi) {
@@ -590,7 +652,8 @@ __global__ void __launch_bounds__(kMaxPassThreads, 2)
     const PassArgs& a = args[lo];
     if (a.active && *a.active == 0) return;
     const long tile = b - tile_prefix[lo];
-    KSum acc = pass_tiles<T, N, RA, RB, P, STRIDED, false>(a, tile, a.ntiles, smem_raw);
+    KSum acc = pass_tiles<T, N, RA, RB, P, STRIDED, false, RC>(a, tile, a.ntiles, smem_raw);
+    pdl_launch_dependents();
     if (a.red.kind != RED_NONE) {
         __syncthreads();
         grid_reduce_finish(acc, reinterpret_cast<double*>(smem_raw), a.red,

@@ -9,11 +9,12 @@ namespace gpue {
 enum Precision : int { PREC_F64 = 0, PREC_F32 = 1 };
 
 struct PassKernel {
-    int n;        // line length
-    int ra, rb;   // radix plan (ra, ra) or (ra, rb, ra)
-    int p;        // threads per line
-    int ls;       // shared-memory line stride (elements per re/im array)
-    int elem;     // bytes per complex element
+    int n;          // line length
+    int ra, rb, rc; // radix plan (ra, ra), (ra, rb, ra) or (ra, rb, rc, ra)
+    int p;          // threads per line
+    int ls;         // shared-memory line stride (elements per re/im array)
+    int elem;       // bytes per complex element
+    int max_threads; // CTA size the kernels are compiled for
     void (*row)(PassArgs);
     void (*col)(PassArgs);
     void (*row_ext)(PassArgs);  // with table / expression factor forms
@@ -34,10 +35,14 @@ const PassKernel* pass_table_f32_b(int* count);
 const PassKernel* pass_table_f64_a(int* count);
 const PassKernel* pass_table_f64_b(int* count);
 
-#define GPUE_PLAN(T, N, RA, RB, P)                                                        \
-    PassKernel{N, RA, RB, P, LineFFT<T, N, RA, RB, P>::LS, (int)sizeof(cx<T>),            \
-               &k_pass<T, N, RA, RB, P, false, false>, &k_pass<T, N, RA, RB, P, true, false>, \
-               &k_pass<T, N, RA, RB, P, false, true>, &k_pass<T, N, RA, RB, P, true, true>,     \
-               &k_pass_batch<T, N, RA, RB, P, false>, &k_pass_batch<T, N, RA, RB, P, true>}
+#define GPUE_PLAN4(T, N, RA, RB, RC, P, MAXT, MINB)                                        \
+    PassKernel{N, RA, RB, RC, P, LineFFT<T, N, RA, RB, P, RC>::LS, (int)sizeof(cx<T>), MAXT,   \
+               &k_pass<T, N, RA, RB, P, false, false, RC, MAXT, MINB>,                       \
+               &k_pass<T, N, RA, RB, P, true, false, RC, MAXT, MINB>,                        \
+               &k_pass<T, N, RA, RB, P, false, true, RC, MAXT, MINB>,                        \
+               &k_pass<T, N, RA, RB, P, true, true, RC, MAXT, MINB>,                         \
+               &k_pass_batch<T, N, RA, RB, P, false, RC, MAXT, MINB>,                        \
+               &k_pass_batch<T, N, RA, RB, P, true, RC, MAXT, MINB>}
+#define GPUE_PLAN(T, N, RA, RB, P) GPUE_PLAN4(T, N, RA, RB, 0, P, kMaxPassThreads, 2)
 
 }  // namespace gpue
