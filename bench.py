@@ -10,11 +10,12 @@ imaginary-time relaxation of the same Hamiltonian on the GPU (done before
 timing) times exp(i theta), theta = 2 pi U(0,1) smoothed by a Gaussian of width
 0.5 (seed 2).
 
-One bench step = 2 split-operator time steps (one full cycle of GPUE's
-alternating x/y gauge order), run by the fused complex64 form through the C
-ABI.  L2 (126 MB) is flushed by a 256 MiB write before every timed step;
-each step is timed with CUDA events on the library's stream.  The same
-protocol times the plain FP64 form for the fused-FP32 vs plain-FP64 ratio.
+One bench step = one gpue_evolve call of 100 split-operator time steps
+(GPUE's default printSteps segment, an even number so both x/y gauge orders
+occur equally), run by the fused complex64 form through the C ABI.  L2
+(126 MB) is flushed by a 256 MiB write before every timed step; each step is
+timed with CUDA events on the library's stream.  The same protocol times the
+plain FP64 form for the fused-FP32 vs plain-FP64 ratio.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -41,19 +42,19 @@ WORK = dict(dim=2, n=1024, box=16.0, wx=1.0, wy=1.0, g=500.0, omega=0.7, gauge=T
             dt=5e-5, gdt=1e-4, total_steps=20000)
 WORKLOAD_NAME = ("2D real-time rotating condensate 1024^2 on [-16,16)^2, g=500, Omega=0.7 "
                  "gauge, dt=5e-5")
-STEPS_PER_BENCH_STEP = 2
+STEPS_PER_BENCH_STEP = 100
 FLUSH_BYTES = 256 << 20
 
 
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1000)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="skip the steady-state and e2e legs")
-    ap.add_argument("--only", choices=["batch", "serve"], default=None,
+    ap.add_argument("--only", choices=["batch", "serve", "large"], default=None,
                     help="run one auxiliary leg alone and print its JSON")
     ap.add_argument("--profile", choices=["fp32", "fp64"], default=None,
                     help="profiling case for ncu: the same workload without the relaxation "
@@ -99,6 +100,9 @@ def work_params(G, precision, device):
 # ------------------------------------------------------------ clocks ------
 
 class ClockSampler:
+    """nvidia-smi clocks and throttle reasons every 50 ms from a reader
+    thread; mark() brackets the timed region, stop() returns the samples
+    taken inside it."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -106,43 +110,65 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.lines = []
+        self.window = [None, None]
 
     def start(self):
+        import threading
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+            return
+
+        def reader():
+            for line in self.proc.stdout:
+                self.lines.append((time.perf_counter(), line))
+
+        self.thread = threading.Thread(target=reader, daemon=True)
+        self.thread.start()
+        t_end = time.perf_counter() + 5.0
+        while not self.lines and time.perf_counter() < t_end:  # first sample seen
+            time.sleep(0.01)
+
+    def mark(self, which):
+        self.window[which] = time.perf_counter()
 
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
-        out, _ = self.proc.communicate(timeout=10)
-        sm, smax, reasons = [], None, set()
+        self.thread.join(timeout=10)
+        t0, t1 = self.window
+        inside = [ln for t, ln in self.lines if t0 is None or (t0 <= t <= t1 + 0.06)]
+        sm, smax, reasons, power = [], None, set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in out.strip().splitlines():
+        for line in inside:
             f = [t.strip() for t in line.split(",")]
             if len(f) < 9:
                 continue
             try:
                 sm.append(float(f[1]))
                 smax = float(f[2])
+                power.append(float(f[3]))
             except ValueError:
                 continue
             for nm, v in zip(names, f[5:9]):
                 if v.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "power_w": statistics.median(power) if power else None,
+                "reasons": sorted(reasons), "samples": len(sm),
+                "window_s": (t1 - t0) if t0 is not None and t1 is not None else None}
 
 
 # ------------------------------------------------------- GPU timing -------
 
 def timed_steps(G, torch, s, steps, warmup, dev, flush, barrier, sampler=None):
-    """Per bench step: flush L2, then 2 time steps between CUDA events."""
+    """Per bench step: flush L2, then one 100-time-step evolve between CUDA events."""
     stream = torch.cuda.ExternalStream(s.stream(), device=dev)
     launches = 0
     off = 0
@@ -158,6 +184,7 @@ def timed_steps(G, torch, s, steps, warmup, dev, flush, barrier, sampler=None):
           for _ in range(steps)]
     if sampler:
         sampler.start()
+        sampler.mark(0)
     for k in range(steps):
         with torch.cuda.stream(stream):
             flush.fill_(float(k & 7))
@@ -168,6 +195,8 @@ def timed_steps(G, torch, s, steps, warmup, dev, flush, barrier, sampler=None):
         with torch.cuda.stream(stream):
             ev[k][1].record(stream)
     torch.cuda.synchronize(dev)
+    if sampler:
+        sampler.mark(1)
     clocks = sampler.stop() if sampler else None
     barrier()
     torch.cuda.synchronize(dev)
@@ -290,7 +319,7 @@ def batch_leg(G, dev, steps=BATCH_STEPS):
         for s, p in zip(solvers, psi0):
             s.set_wfc(p)
         with G.Batch(solvers) as b:
-            b.evolve(0, 2 * BATCH["every"] + 1, **kw)  # captures the graphs
+            b.evolve(0, 2 * BATCH["every"] + 1, autotune=True, **kw)  # tunes, captures graphs
             for s, p in zip(solvers, psi0):
                 s.set_wfc(p)
             res, st = b.evolve(0, steps, **kw)
@@ -317,6 +346,62 @@ def batch_leg(G, dev, steps=BATCH_STEPS):
                       "absolute stop; none is expected to stop this early), complex64 with "
                       "FP64 reductions; sequential = the same solves through gpue_evolve one "
                       "after another (sum of their device times)" % (steps - 1)}
+
+
+# ---------------------------------------------------- large 3D ground state
+
+# 256^3 on [-12,12)^3, (wx,wy,wz) = (1,1,4), g = 1000, dt = 1e-4, 5000
+# imaginary-time steps from a Gaussian of width 1 times (1 + 0.01 xi) (seed
+# 3); the fused form then polishes with 50 FP64 steps.  The field (128 MiB
+# complex64, 256 MiB complex128) does not fit in L2, so this is the case the
+# HBM roofline describes.
+LARGE = dict(n=256, box=12.0, wz=4.0, g=1000.0, gdt=1e-4, steps=5000, polish=50, seed=3)
+
+
+def large_leg(G, dev, peak):
+    n = LARGE["n"]
+    psi0 = gauss_start(3, n, LARGE["box"], LARGE["seed"])
+    pts = n ** 3
+    out = {"workload": "3D imaginary-time ground state 256^3 on [-12,12)^3, (1,1,4) trap, "
+                       "g=1000, dt=1e-4, 5000 steps (+50 FP64 polish steps for the fused form)"}
+
+    def params(prec):
+        return G.make_params(3, n, LARGE["box"], wz=LARGE["wz"], g=LARGE["g"], gdt=LARGE["gdt"],
+                             precision=prec, device=dev)
+
+    with G.Solver(params(G.PREC_FP64)) as s:
+        plans64 = s.autotune()
+        s.set_wfc(psi0)
+        r = s.evolve(LARGE["steps"], 0)
+        E64 = s.energy()
+        s.evolve(LARGE["polish"], 0, step_offset=LARGE["steps"])
+        E64p = s.energy()
+    t64 = r["device_ms"] * 1e-3 / LARGE["steps"]
+    with G.Solver(params(G.PREC_FP32)) as s:
+        plans32 = s.autotune()
+        s.set_wfc(psi0)
+        r = s.evolve(LARGE["steps"], 0)
+        E32 = s.energy()
+        s.evolve(0, 0, polish_steps=LARGE["polish"], step_offset=LARGE["steps"])
+        E32p = s.energy()
+    t32 = r["device_ms"] * 1e-3 / LARGE["steps"]
+    # 5 full-field read+write passes per 3D step (no gauge): 2*5*s bytes per point
+    out.update({
+        "fp32_value": pts / t32, "fp64_value": pts / t64, "unit": UNIT,
+        "fp32_over_fp64": t64 / t32,
+        "fp32_roofline_frac": 2 * 5 * 8 * pts / t32 / 1e9 / peak,
+        "fp64_roofline_frac": 2 * 5 * 16 * pts / t64 / 1e9 / peak,
+        "E_fp64": E64, "E_fp32": E32, "dE_rel_fp32": abs(E32 - E64) / abs(E64),
+        "E_fp64_5050": E64p, "E_fp32_polished": E32p,
+        "dE_rel_fp32_polished": abs(E32p - E64p) / abs(E64p),
+        "plans_fp32": [(p["ra"], p["rb"], p["threads_per_line"], p["lines_per_cta"])
+                       for p in plans32],
+        "plans_fp64": [(p["ra"], p["rb"], p["threads_per_line"], p["lines_per_cta"])
+                       for p in plans64],
+        "note": "steady-state device time of one gpue_evolve call of 5000 steps per form "
+                "(graph-replayed, renormalised every step); roofline bytes 2*5*8 (complex64) "
+                "or 2*5*16 (complex128) per point and step against the measured HBM copy rate"})
+    return out
 
 
 # -------------------------------------------------------------- serving ---
@@ -369,7 +454,8 @@ def serve_leg(G, dev):
     psi0 = [gauss_start(q["dim"], q["n"], q["box"], q["seed"]) for q in reqs]
     results = {}
     with G.Server(precision=G.PREC_FP32, check_steps=SERVE["check"], threshold=SERVE["thr"],
-                  threshold_abs=True, hbm_budget=SERVE["budget"], device=dev) as srv:
+                  threshold_abs=True, hbm_budget=SERVE["budget"], device=dev,
+                  autotune=True) as srv:
         t0 = time.perf_counter()
 
         def submitter():
@@ -486,6 +572,15 @@ def reference_arm(args):
 
 # ------------------------------------------------------------- main -------
 
+def measured_peak():
+    """HBM copy bandwidth (GB/s) from MEASURED_PEAKS.json, else the fallback."""
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
 def profile_case(args):
     """Small deterministic run for ncu captures (same kernels as the timed leg)."""
     import numpy as np
@@ -498,9 +593,10 @@ def profile_case(args):
     prec = G.PREC_FP32 if args.profile == "fp32" else G.PREC_FP64
     with G.Solver(work_params(G, prec, 0)) as s:
         s.set_wfc(psi0)
-        r0 = s.evolve(args.warmup * STEPS_PER_BENCH_STEP, 1)
-        r1 = s.evolve(args.steps * STEPS_PER_BENCH_STEP, 1,
-                      step_offset=args.warmup * STEPS_PER_BENCH_STEP)
+        # here a step is 2 time steps (one x/y gauge-order cycle), so that
+        # captures can pick single launches out of a short run
+        r0 = s.evolve(args.warmup * 2, 1)
+        r1 = s.evolve(args.steps * 2, 1, step_offset=args.warmup * 2)
     print(json.dumps({"profile": args.profile, "warmup_launches": r0["kernel_launches"],
                       "launches": r1["kernel_launches"], "device_ms": r1["device_ms"]}))
 
@@ -516,8 +612,11 @@ def main():
     import torch
     import gpue_b200 as G
     if args.only:
-        leg = batch_leg if args.only == "batch" else serve_leg
-        print(json.dumps({args.only: leg(G, 0)}), flush=True)
+        if args.only == "large":
+            print(json.dumps({"large": large_leg(G, 0, measured_peak()[0])}), flush=True)
+        else:
+            leg = batch_leg if args.only == "batch" else serve_leg
+            print(json.dumps({args.only: leg(G, 0)}), flush=True)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -539,8 +638,11 @@ def main():
     psi0 = initial_state(G, dev)
     pts = WORK["n"] ** 2
     res = {}
+    plans = {}
     for name, prec in (("fp64", G.PREC_FP64), ("fp32", G.PREC_FP32)):
         with G.Solver(work_params(G, prec, dev)) as s:
+            plans[name] = [(p["ra"], p["rb"], p["threads_per_line"], p["lines_per_cta"])
+                           for p in s.autotune()]  # later solvers of this shape reuse it
             s.set_wfc(psi0)
             sampler = ClockSampler(dev) if name == "fp32" else None
             ms, launches, clocks = timed_steps(G, torch, s, args.steps, args.warmup, dev, flush,
@@ -564,12 +666,7 @@ def main():
             dist.destroy_process_group()
         return
 
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
-    except Exception:
-        peak, peak_src = 6650.0, "fallback"
+    peak, peak_src = measured_peak()
     # algorithmic bytes: P = 4 full-field read+write passes per time step for
     # 2D with the gauge, complex64 (8 B): 2*4*8 = 64 B per grid point and step
     alg_bytes_per_step = 2 * 4 * 8 * pts
@@ -596,6 +693,7 @@ def main():
     acc = accuracy_leg(G, psi0, dev)
     batched = None if args.quick else batch_leg(G, dev)
     served = None if args.quick else serve_leg(G, dev)
+    large = None if args.quick else large_leg(G, dev, peak)
     line = {
         "metric": METRIC, "value": v32, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": res["fp32"]["ms"] / args.steps,
@@ -603,9 +701,11 @@ def main():
         "data": "synthetic (seeded; FP64 imaginary-time relaxed state x smoothed random phase)",
         "config": {"workload": WORKLOAD_NAME, "grid": WORK["n"], "form": "fused complex64, "
                    "FP64 operator phases rounded, FP64 reductions",
-                   "step": "%d split-operator time steps (one x/y gauge-order cycle)"
-                           % STEPS_PER_BENCH_STEP,
-                   "l2": "flushed before every timed step (256 MiB write)",
+                   "step": "one gpue_evolve call of %d split-operator time steps (GPUE's "
+                           "printSteps segment)" % STEPS_PER_BENCH_STEP,
+                   "l2": "flushed before every timed step (256 MiB write); the 8 MiB field "
+                         "stays L2-resident within a step, as in a 20000-step run",
+                   "plans": plans,
                    "parallelism": "replicas" if world > 1 else "single"},
         "plain_fp64": {"value": v64, "ms_per_step": res["fp64"]["ms"] / args.steps,
                        "fused_fp32_over_plain_fp64": v32 / v64},
@@ -613,7 +713,7 @@ def main():
                          "note": "one gpue_evolve call of 20000 steps (the configuration's "
                                  "length), graph-replayed, no L2 flush"},
         "accuracy": acc,
-        "batched_sweep": batched, "serving": served,
+        "batched_sweep": batched, "serving": served, "large_3d": large,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
         "clocks": res["fp32"]["clocks"],
         "gpu_launches": res["fp32"]["launches"],

@@ -14,7 +14,7 @@ import numpy as np
 
 __all__ = ["lib", "Params", "EvolveOpts", "EvolveResult", "Solver", "GpueError", "Batch",
            "BatchOpts", "BatchResult", "BatchStats", "Server", "ServerOpts", "Request",
-           "ServerResult", "ServerStats",
+           "ServerResult", "ServerStats", "PlanInfo",
            "PREC_FP64", "PREC_FP32", "C128", "C64", "MEM_HOST", "MEM_DEVICE",
            "GAUGE_ROTATION", "GAUGE_CONSTANT", "supported_length", "default_params"]
 
@@ -72,7 +72,7 @@ class BatchOpts(C.Structure):
     _fields_ = [("energy_calc_steps", C.c_int32), ("energy_calc_threshold", C.c_double),
                 ("threshold_abs", C.c_int32), ("max_steps", C.c_int32),
                 ("norm_guard", C.c_int32), ("segments_per_launch", C.c_int32),
-                ("reserved", C.c_int32 * 6)]
+                ("autotune", C.c_int32), ("reserved", C.c_int32 * 5)]
 
 
 class BatchResult(C.Structure):
@@ -90,11 +90,22 @@ class BatchStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class PlanInfo(C.Structure):
+    _fields_ = [("n", C.c_int32), ("ra", C.c_int32), ("rb", C.c_int32), ("rc", C.c_int32),
+                ("threads_per_line", C.c_int32), ("lines_per_cta", C.c_int32),
+                ("threads", C.c_int32), ("blocks", C.c_int32), ("tuned", C.c_int32),
+                ("us", C.c_float), ("default_us", C.c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class ServerOpts(C.Structure):
     _fields_ = [("device", C.c_int32), ("precision", C.c_int32),
                 ("hbm_budget_bytes", C.c_int64), ("check_steps", C.c_int32),
                 ("max_active", C.c_int32), ("threshold", C.c_double),
-                ("threshold_abs", C.c_int32), ("reserved", C.c_int32 * 7)]
+                ("threshold_abs", C.c_int32), ("autotune", C.c_int32),
+                ("reserved", C.c_int32 * 6)]
 
 
 class Request(C.Structure):
@@ -162,6 +173,8 @@ def lib():
         L.gpue_batch_last_error.restype = C.c_char_p
         L.gpue_batch_evolve.argtypes = [vp, i32, C.POINTER(BatchOpts), C.POINTER(BatchResult),
                                         C.POINTER(BatchStats)]
+        L.gpue_autotune.argtypes = [vp, i32]
+        L.gpue_get_plan.argtypes = [vp, i32, C.POINTER(PlanInfo)]
         L.gpue_server_create.argtypes = [C.POINTER(ServerOpts), C.POINTER(vp)]
         L.gpue_server_destroy.argtypes = [vp]
         L.gpue_server_last_error.argtypes = [vp]
@@ -179,7 +192,8 @@ def lib():
                      "gpue_set_operators", "gpue_set_wfc", "gpue_get_wfc", "gpue_evolve",
                      "gpue_energy", "gpue_norm", "gpue_ctx_stream", "gpue_ctx_wfc_device",
                      "gpue_load_param_text", "gpue_ast_parse", "gpue_batch_create",
-                     "gpue_batch_destroy", "gpue_batch_evolve"):
+                     "gpue_batch_destroy", "gpue_batch_evolve", "gpue_autotune",
+                     "gpue_get_plan"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -320,6 +334,16 @@ class Solver:
         self._ck(lib().gpue_ctx_wfc_device(self._h, C.byref(p), C.byref(d)))
         return p.value, d.value
 
+    def autotune(self, force=False):
+        """Time the compiled plans and lines-per-CTA choices; keep the fastest."""
+        self._ck(lib().gpue_autotune(self._h, 1 if force else 0))
+        return [self.plan(a) for a in range(len(self.shape))]
+
+    def plan(self, axis):
+        out = PlanInfo()
+        self._ck(lib().gpue_get_plan(self._h, axis, C.byref(out)))
+        return out.as_dict()
+
     def load_param_text(self, text, time_mode=0, doubles=None):
         """Parameter-file fields (GPUE's -I file) from "name = expr" lines."""
         doubles = doubles or {}
@@ -359,9 +383,10 @@ class Batch:
         self.close()
 
     def evolve(self, gstate, max_steps, energy_every=0, threshold=-1.0, threshold_abs=False,
-               norm_guard=-1, segments_per_launch=0):
+               norm_guard=-1, segments_per_launch=0, autotune=False):
         """Returns (per-solve result dicts, stats dict)."""
         o = BatchOpts()
+        o.autotune = 1 if autotune else 0
         o.energy_calc_steps = energy_every
         o.energy_calc_threshold = threshold
         o.threshold_abs = 1 if threshold_abs else 0
@@ -383,8 +408,9 @@ class Server:
     buffer are kept referenced here until its result has been polled."""
 
     def __init__(self, precision=PREC_FP32, check_steps=100, threshold=1e-10,
-                 threshold_abs=True, hbm_budget=0, max_active=0, device=0):
+                 threshold_abs=True, hbm_budget=0, max_active=0, device=0, autotune=False):
         o = ServerOpts()
+        o.autotune = 1 if autotune else 0
         o.device = device
         o.precision = precision
         o.hbm_budget_bytes = int(hbm_budget)

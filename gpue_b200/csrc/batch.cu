@@ -33,6 +33,12 @@ std::string pass_signature(const gpue_ctx* c, int prec, const std::vector<LPass>
     for (int a = 0; a < c->dim; ++a) {
         const LaunchCfg& lc = c->lc[prec][a];
         put(c->ax[a].n);
+        if (lc.k) {
+            put(lc.k->ra);
+            put(lc.k->rb);
+            put(lc.k->rc);
+            put(lc.k->p);
+        }
         put(lc.threads);
         put(lc.ntiles);
         put((long)lc.smem);
@@ -481,6 +487,7 @@ gpue_status gpue_batch_evolve(gpue_batch* b, int32_t gstate, const gpue_batch_op
                                            (o.norm_guard < 0 && c->prec == GPUE_PREC_FP32));
         r.guard[i] = guard;
         BCTX(c, unpolish(c));
+        if (o.autotune) BCTX(c, autotune_ctx(c, c->prec, false));
         BCTX(c, build_tables(c, c->prec, gstate));
         BCTX(c, apply_pending_scale(c, c->prec));
         if (guard) {

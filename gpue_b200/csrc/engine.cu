@@ -22,6 +22,8 @@
 // authoritative one until the next FP32 evolve.
 
 
+#include <cstdlib>
+
 #include "engine_internal.h"
 
 using namespace gpue;
@@ -194,44 +196,100 @@ gpue_status build_tables(gpue_ctx* c, int prec, int gstate) {
 
 // ---------------------------------------------------------------- passes --
 
-// Launch shape for one precision and axis: C lines per tile, a persistent
-// grid of (resident CTAs per SM) x SMs walking the tiles.
-gpue_status plan_axis(gpue_ctx* c, int prec, int axis) {
-    LaunchCfg& lc = c->lc[prec][axis];
-    const int n = c->ax[axis].n;
-    const PassKernel* k = find_pass_kernel(kprec(prec), n);
-    if (!k) return fail(c, GPUE_ERR_UNSUPPORTED, "no FFT plan for length %d", n);
-    const long nlines = c->N / n;
+// Launch shape of plan k with C lines per tile and a persistent grid of
+// (resident CTAs per SM) x SMs walking the tiles; false when C does not fit.
+bool build_cfg(gpue_ctx* c, int prec, int axis, const PassKernel* k, int C, LaunchCfg& lc) {
+    const long nlines = c->N / c->ax[axis].n;
+    if (C < 1 || C * k->p > k->max_threads || nlines % C) return false;
+    if (axis > 0 && c->ax[0].n % C) return false;  // a tile's lines are adjacent in x
+    size_t smem = (size_t)C * k->ls * k->elem;
+    const size_t red_need = 2 * ((C * k->p + 31) / 32) * sizeof(double);
+    if (smem < red_need) smem = red_need;
+    int max_smem = 48 * 1024;
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+    if (smem > (size_t)max_smem) return false;
+    void* fns[4] = {(void*)k->row, (void*)k->col, (void*)k->row_batch, (void*)k->col_batch};
+    if (smem > 48 * 1024)
+        for (void* f : fns)
+            if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+                cudaSuccess)
+                return false;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, axis == 0 ? fns[0] : fns[1],
+                                                      C * k->p, smem) != cudaSuccess)
+        return false;
+    if (per_sm < 1) return false;
+    lc = LaunchCfg();
+    lc.k = k;
+    lc.lines = C;
+    lc.threads = C * k->p;
+    lc.ntiles = nlines / C;
+    lc.smem = smem;
+    long blocks = (long)per_sm * c->sms;
+    if (blocks > lc.ntiles) blocks = lc.ntiles;
+    lc.blocks = (int)blocks;
+    return true;
+}
+
+// Lines per tile without tuning: 128 threads per tile for rows; for strided
+// passes at least one 32-byte sector per row.
+int default_lines(const gpue_ctx* c, int axis, const PassKernel* k) {
+    const long nlines = c->N / c->ax[axis].n;
     int C;
     if (axis == 0) {
         C = 128 / k->p;
         if (C < 1) C = 1;
     } else {
-        const int min_c = (32 + k->elem - 1) / k->elem;  // one 32-byte sector per row
+        const int min_c = (32 + k->elem - 1) / k->elem;
         C = 128 / k->p;
         if (C < min_c) C = min_c;
         if (C * k->p > k->max_threads) C = k->max_threads / k->p;
         while (C > 1 && c->ax[0].n % C) C >>= 1;
     }
     while (C > 1 && nlines % C) C >>= 1;
-    lc.k = k;
-    lc.threads = C * k->p;
-    lc.ntiles = nlines / C;
-    lc.smem = (size_t)C * k->ls * k->elem;
-    const size_t red_need = 2 * ((lc.threads + 31) / 32) * sizeof(double);
-    if (lc.smem < red_need) lc.smem = red_need;
-    void* fn = axis == 0 ? (void*)k->row : (void*)k->col;
-    if (lc.smem > 48 * 1024)
-        CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lc.smem));
-    int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, lc.threads, lc.smem));
-    if (per_sm < 1) per_sm = 1;
-    long blocks = (long)per_sm * c->sms;
-    if (blocks > lc.ntiles) blocks = lc.ntiles;
-    lc.blocks = (int)blocks;
-    return GPUE_OK;
+    return C;
 }
 
+struct TuneKey {
+    int prec, dim, n, axis;
+    bool operator<(const TuneKey& o) const { return std::memcmp(this, &o, sizeof o) < 0; }
+};
+struct TuneChoice {
+    int ra, rb, rc, p, lines;
+    float us, default_us;
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneChoice> g_tune;  // per process, guarded by g_tune_mu
+
+bool cached_choice(const gpue_ctx* c, int prec, int axis, TuneChoice& out) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(TuneKey{prec, c->dim, c->ax[axis].n, axis});
+    if (it == g_tune.end()) return false;
+    out = it->second;
+    return true;
+}
+
+gpue_status plan_axis(gpue_ctx* c, int prec, int axis) {
+    LaunchCfg& lc = c->lc[prec][axis];
+    const int n = c->ax[axis].n;
+    const PassKernel* ks[8];
+    const int nk = find_pass_kernels(kprec(prec), n, ks, 8);
+    if (!nk) return fail(c, GPUE_ERR_UNSUPPORTED, "no FFT plan for length %d", n);
+    TuneChoice tc;
+    if (cached_choice(c, prec, axis, tc)) {
+        for (int i = 0; i < nk; ++i)
+            if (ks[i]->ra == tc.ra && ks[i]->rb == tc.rb && ks[i]->rc == tc.rc &&
+                ks[i]->p == tc.p && build_cfg(c, prec, axis, ks[i], tc.lines, lc)) {
+                lc.tuned = true;
+                lc.us = tc.us;
+                lc.default_us = tc.default_us;
+                return GPUE_OK;
+            }
+    }
+    if (!build_cfg(c, prec, axis, ks[0], default_lines(c, axis, ks[0]), lc))
+        return fail(c, GPUE_ERR_CUDA, "no launch shape for length %d", n);
+    return GPUE_OK;
+}
 
 gpue_status make_pass_args(gpue_ctx* c, int prec, const LPass& lp, int gstate, PassArgs& a) {
     const LaunchCfg& lc = c->lc[prec][lp.axis];
@@ -604,6 +662,88 @@ void destroy_graphs(gpue_ctx* c) {
     c->graphs.clear();
 }
 
+// ------------------------------------------------------------- autotune --
+
+// Mean device time of one FFT round-trip pass (forward then inverse along
+// the axis) over a copy of the state, with the current launch shape.
+gpue_status time_roundtrip(gpue_ctx* c, int prec, int axis, float* us) {
+    LPass lp;
+    lp.axis = axis;
+    lp.ops = {OP_FFT_F, OP_FFT_I};
+    lp.from_scratch = true;
+    PassArgs a;
+    gpue_status st = make_pass_args(c, prec, lp, 0, a);
+    if (st) return st;
+    a.active = nullptr;
+    const LaunchCfg& lc = c->lc[prec][axis];
+    void (*fn)(PassArgs) = axis == 0 ? lc.k->row : lc.k->col;
+    // unnormalised round trips grow the values by n per launch: 8 launches
+    // stay far inside the FP32 range for n <= 1024
+    CK(cudaMemcpyAsync(c->scratch, state_of(c, prec), c->N * elem_size(prec),
+                       cudaMemcpyDeviceToDevice, c->stream));
+    for (int w = 0; w < 2; ++w)
+        CK(launch_kernel(fn, lc.blocks, lc.threads, lc.smem, c->stream, false, a));
+    const int reps = 6;
+    CK(cudaEventRecord(c->ev0, c->stream));
+    for (int r = 0; r < reps; ++r)
+        CK(launch_kernel(fn, lc.blocks, lc.threads, lc.smem, c->stream, false, a));
+    CK(cudaEventRecord(c->ev1, c->stream));
+    CK(cudaEventSynchronize(c->ev1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    *us = ms * 1e3f / reps;
+    return GPUE_OK;
+}
+
+gpue_status autotune_ctx(gpue_ctx* c, int prec, bool force) {
+    for (int axis = 0; axis < c->dim; ++axis) {
+        TuneChoice tc;
+        if (!force && cached_choice(c, prec, axis, tc)) {
+            gpue_status st = plan_axis(c, prec, axis);
+            if (st) return st;
+            continue;
+        }
+        const PassKernel* ks[8];
+        const int nk = find_pass_kernels(kprec(prec), c->ax[axis].n, ks, 8);
+        if (!nk) return fail(c, GPUE_ERR_UNSUPPORTED, "no FFT plan for length %d", c->ax[axis].n);
+        LaunchCfg def;
+        if (!build_cfg(c, prec, axis, ks[0], default_lines(c, axis, ks[0]), def))
+            return fail(c, GPUE_ERR_CUDA, "no launch shape for length %d", c->ax[axis].n);
+        c->lc[prec][axis] = def;
+        float def_us = 0.f;
+        gpue_status st = time_roundtrip(c, prec, axis, &def_us);
+        if (st) return st;
+        LaunchCfg best = def;
+        float best_us = def_us;
+        for (int i = 0; i < nk; ++i) {
+            for (int C = 1; C <= 64; C *= 2) {
+                LaunchCfg cand;
+                if (!build_cfg(c, prec, axis, ks[i], C, cand)) continue;
+                if (cand.k == def.k && cand.lines == def.lines) continue;
+                c->lc[prec][axis] = cand;
+                float t0 = 0.f, t1 = 0.f;
+                st = time_roundtrip(c, prec, axis, &t0);
+                if (!st) st = time_roundtrip(c, prec, axis, &t1);
+                if (st) return st;
+                const float t = std::min(t0, t1);
+                if (t < 0.97f * best_us) {  // a clear gain only: noise must not flip plans
+                    best = cand;
+                    best_us = t;
+                }
+            }
+        }
+        best.tuned = true;
+        best.us = best_us;
+        best.default_us = def_us;
+        c->lc[prec][axis] = best;
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune[TuneKey{prec, c->dim, c->ax[axis].n, axis}] =
+            TuneChoice{best.k->ra, best.k->rb, best.k->rc, best.k->p, best.lines, best_us, def_us};
+    }
+    destroy_graphs(c);  // the captured segments hold the old launch shapes
+    return GPUE_OK;
+}
+
 struct LoopOut {
     int done = 0, early = 0, n_en = 0;
     double energy = NAN;
@@ -811,6 +951,11 @@ gpue_status gpue_ctx_create(const gpue_params* p, gpue_ctx** out) {
     if (st) return st;
     for (int a = 0; a < c->dim; ++a) {
         st = plan_axis(c, c->prec, a);
+        if (st) return st;
+    }
+    const char* tune = std::getenv("GPUE_AUTOTUNE");
+    if (tune && tune[0] == '1') {
+        st = autotune_ctx(c, c->prec, false);
         if (st) return st;
     }
     *out = cp.release();
@@ -1066,6 +1211,32 @@ gpue_status gpue_ctx_wfc_device(gpue_ctx* c, void** psi, int32_t* dtype) {
     return GPUE_OK;
 }
 
+gpue_status gpue_autotune(gpue_ctx* c, int32_t flags) {
+    if (!c || (flags & ~1)) return GPUE_ERR_INVALID_ARG;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    return autotune_ctx(c, c->prec, (flags & 1) != 0);
+}
+
+gpue_status gpue_get_plan(gpue_ctx* c, int32_t axis, gpue_plan_info* out) {
+    if (!c || !out || axis < 0 || axis >= c->dim) return GPUE_ERR_INVALID_ARG;
+    const LaunchCfg& lc = c->lc[c->prec][axis];
+    if (!lc.k) return fail(c, GPUE_ERR_STATE, "axis %d not planned", axis);
+    std::memset(out, 0, sizeof *out);
+    out->n = lc.k->n;
+    out->ra = lc.k->ra;
+    out->rb = lc.k->rb;
+    out->rc = lc.k->rc;
+    out->threads_per_line = lc.k->p;
+    out->lines_per_cta = lc.lines;
+    out->threads = lc.threads;
+    out->blocks = lc.blocks;
+    out->tuned = lc.tuned ? 1 : 0;
+    out->us = lc.us;
+    out->default_us = lc.default_us;
+    return GPUE_OK;
+}
+
 gpue_status gpue_evolve(gpue_ctx* c, int32_t nsteps, int32_t gstate,
                         const gpue_evolve_opts* opts, gpue_evolve_result* res) {
     if (!c || nsteps < 0 || (gstate != 0 && gstate != 1)) return GPUE_ERR_INVALID_ARG;
@@ -1159,16 +1330,22 @@ gpue_status gpue_evolve(gpue_ctx* c, int32_t nsteps, int32_t gstate,
 
 namespace gpue {
 
-const PassKernel* find_pass_kernel(int prec, int n) {
+int find_pass_kernels(int prec, int n, const PassKernel** out, int cap) {
+    int k = 0;
     for (int part = 0; part < 2; ++part) {
         int cnt = 0;
         const PassKernel* t =
             prec == PREC_F32 ? (part ? pass_table_f32_b(&cnt) : pass_table_f32_a(&cnt))
                              : (part ? pass_table_f64_b(&cnt) : pass_table_f64_a(&cnt));
         for (int i = 0; i < cnt; ++i)
-            if (t[i].n == n) return &t[i];
+            if (t[i].n == n && k < cap) out[k++] = &t[i];
     }
-    return nullptr;
+    return k;
+}
+
+const PassKernel* find_pass_kernel(int prec, int n) {
+    const PassKernel* k = nullptr;
+    return find_pass_kernels(prec, n, &k, 1) ? k : nullptr;
 }
 
 }  // namespace gpue

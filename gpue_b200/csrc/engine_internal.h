@@ -12,6 +12,7 @@
 #include <cstring>
 #include <functional>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <string>
 #include <vector>
@@ -49,8 +50,11 @@ struct Tables {
 struct LaunchCfg {
     const PassKernel* k = nullptr;
     int threads = 0, blocks = 0;
+    int lines = 0;          // lines per tile (CTA)
     long ntiles = 0;
     size_t smem = 0;
+    bool tuned = false;     // chosen by the autotuner
+    float us = 0, default_us = 0;  // tuned and default pass times (FFT round trip)
 };
 
 struct GraphKey {
@@ -184,6 +188,9 @@ void* state_of(gpue_ctx* c, int prec);
 bool axis_gauge_active(const gpue_ctx* c, int axis);
 gpue_status build_tables(gpue_ctx* c, int prec, int gstate);
 gpue_status plan_axis(gpue_ctx* c, int prec, int axis);
+// Times every compiled plan and lines-per-CTA choice for the context's grid
+// and keeps the fastest for each axis (cached per shape for the process).
+gpue_status autotune_ctx(gpue_ctx* c, int prec, bool force);
 gpue_status make_pass_args(gpue_ctx* c, int prec, const LPass& lp, int gstate, PassArgs& a);
 void step_passes(gpue_ctx* c, int i, int gstate, bool scale_first, double rexp, bool guard,
                  std::vector<LPass>& out);

@@ -1,17 +1,22 @@
 // kernels_f32_b.cu -- complex64 pass kernels (the fused FP32 form), lengths >= 256.
 //
-// One plan per line length: radix sequence (RA, RA) or (RA, RB, RA) and P
-// threads per line, chosen for E = N/P <= 16 complex values per thread where
-// the length allows it (more resident warps, shorter straight-line code).
+// Plans per line length: radix sequence (RA, RA) or (RA, RB, RA) and P
+// threads per line, for E = N/P <= 16 complex values per thread where the
+// length allows it (more resident warps, shorter straight-line code).  The
+// first plan of a length is the default; the others (fewer threads per line,
+// so a strided pass can take more lines per CTA and read whole 128-byte rows)
+// are candidates for the autotuner.
 #include "registry.h"
 
 namespace gpue {
 
 static const PassKernel kTable[] = {
     GPUE_PLAN(float, 256, 8, 4, 32),
+    GPUE_PLAN(float, 256, 16, 0, 16),
     GPUE_PLAN(float, 320, 4, 20, 16),
     GPUE_PLAN(float, 384, 4, 24, 16),
     GPUE_PLAN(float, 512, 8, 8, 64),
+    GPUE_PLAN(float, 512, 8, 8, 32),
     GPUE_PLAN(float, 640, 8, 10, 16),
     GPUE_PLAN(float, 768, 8, 12, 32),
     GPUE_PLAN(float, 1024, 16, 4, 64),

@@ -3,6 +3,7 @@
 // One plan per line length: radix sequence (RA, RA) or (RA, RB, RA) and P
 // threads per line, chosen for E = N/P <= 16 complex values per thread where
 // the length allows it (more resident warps, shorter straight-line code).
+// Their P <= 16 already lets a strided pass read whole 128-byte rows.
 #include "registry.h"
 
 namespace gpue {

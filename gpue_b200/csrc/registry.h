@@ -23,8 +23,10 @@ struct PassKernel {
     void (*col_batch)(const PassArgs*, const long*, int);
 };
 
-// nullptr when the length has no compiled plan
+// The default plan for a length; nullptr when none is compiled
 const PassKernel* find_pass_kernel(int prec, int n);
+// All plans for a length, default first; returns how many (at most cap)
+int find_pass_kernels(int prec, int n, const PassKernel** out, int cap);
 // supported line lengths, ascending; returns the count
 int supported_lengths(int prec, const int** out);
 

@@ -171,6 +171,30 @@ gpue_status gpue_ast_parse(const char* expr, const char* const* names, const dou
 /* Device pointer of the resident wavefunction and its dtype (GPUE_C128/C64). */
 gpue_status gpue_ctx_wfc_device(gpue_ctx* ctx, void** psi, int32_t* dtype);
 
+/* No counterpart in GPUE (which hands its transforms to cuFFT plans,
+ * src/ds.cu:11-79): choose, by timing on this device, the FFT radix plan and
+ * the lines per CTA of every axis of the context's grid.  Each compiled plan
+ * of the axis length and each lines-per-CTA count that fits is timed on a
+ * forward/inverse round trip over a copy of the state; the fastest (by a
+ * clear margin over the default) is kept.  Choices are cached per (precision,
+ * dimension, length, axis) for the process, so later contexts of the same
+ * shape reuse them without timing; flags bit 0 re-times a cached shape.
+ * Setting GPUE_AUTOTUNE=1 in the environment makes gpue_ctx_create do this. */
+gpue_status gpue_autotune(gpue_ctx* ctx, int32_t flags);
+
+typedef struct gpue_plan_info {
+    int32_t n;                     /* line length */
+    int32_t ra, rb, rc;            /* radix sequence (ra, [rb, [rc,]] ra) */
+    int32_t threads_per_line;
+    int32_t lines_per_cta;
+    int32_t threads, blocks;       /* CTA size and persistent grid */
+    int32_t tuned;                 /* 1 if chosen by gpue_autotune */
+    float us, default_us;          /* round-trip pass times measured by the tuner */
+} gpue_plan_info;
+
+/* The launch shape the context uses along an axis (0 = x). */
+gpue_status gpue_get_plan(gpue_ctx* ctx, int32_t axis, gpue_plan_info* out);
+
 /* No counterpart in GPUE: sum |psi|^2 * dV of a wavefunction the caller owns
  * on the current device, written to *out (device memory the caller owns),
  * for callers that must not trigger any device allocation, such as a server
@@ -205,7 +229,8 @@ typedef struct gpue_batch_opts {
     int32_t max_steps;             /* steps per solve at most (>= 1) */
     int32_t norm_guard;            /* as gpue_evolve_opts.norm_guard */
     int32_t segments_per_launch;   /* check segments per graph launch; 0 = automatic */
-    int32_t reserved[6];
+    int32_t autotune;              /* 1: gpue_autotune every solve first (cached per shape) */
+    int32_t reserved[5];
 } gpue_batch_opts;
 
 typedef struct gpue_batch_result {
@@ -250,7 +275,8 @@ typedef struct gpue_server_opts {
     int32_t max_active;        /* resident solves at most; 0: no limit */
     double threshold;          /* imaginary-time stop between consecutive checks */
     int32_t threshold_abs;     /* 1: |E_old-E| < threshold; 0: |E_old-E| < threshold*E_old */
-    int32_t reserved[7];
+    int32_t autotune;          /* 1: gpue_autotune each admitted solve (cached per shape) */
+    int32_t reserved[6];
 } gpue_server_opts;
 
 typedef struct gpue_request {
