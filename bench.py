@@ -35,6 +35,8 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from gpue_b200 import replicas  # noqa: E402  (pure Python; loads no library)
+
 METRIC = ("grid-point-steps/s fused-FP32 vs plain-FP64 (same B200, ΔE/E≤1e-6); "
           "p99 lat")
 UNIT = "grid-point-steps/s"
@@ -210,7 +212,7 @@ def steady_state(G, s, nsteps):
     return r["device_ms"], r["kernel_launches"]
 
 
-def e2e_leg(G, torch, psi0, dev, calls=10, steps_per_call=100):
+def e2e_leg(G, torch, psi0, dev, calls=10, steps_per_call=100, dist=None):
     """Through the C ABI with pinned host buffers: upload psi (complex128),
     evolve one printSteps-sized segment, download psi and the energy."""
     import numpy as np
@@ -244,7 +246,9 @@ def e2e_leg(G, torch, psi0, dev, calls=10, steps_per_call=100):
         torch.cuda.synchronize(dev)
         ms = e0.elapsed_time(e1)
     pts = n * n
-    return {"value": pts * steps_per_call * calls / (ms * 1e-3), "unit": UNIT,
+    rate, _, secs = replicas.job_rate(pts * steps_per_call * calls, ms * 1e-3, dist, dev)
+    ms = secs * 1e3
+    return {"value": rate, "unit": UNIT,
             "h2d_bytes_per_step": pts * 16, "d2h_bytes_per_step": pts * 16 + 8,
             "step": "one gpue_evolve() call of %d time steps (GPUE's default printSteps) "
                     "with psi uploaded from pinned host memory before it and psi plus the "
@@ -303,10 +307,14 @@ def batch_cases():
     return out
 
 
-def batch_leg(G, dev, steps=BATCH_STEPS):
+def batch_leg(G, dev, steps=BATCH_STEPS, dist=None):
     """The 96 solves as one gpue_batch against the same solves run one after
-    another through gpue_evolve (same form, same checks)."""
-    cs = batch_cases()
+    another through gpue_evolve (same form, same checks).  Under several
+    ranks each GPU takes every world-th solve (no communication) and the
+    rates are all ranks' point-steps over the slowest rank's time."""
+    world = dist.get_world_size() if dist is not None else 1
+    rank = dist.get_rank() if dist is not None else 0
+    cs = [batch_cases()[i] for i in replicas.shard(BATCH["solves"], world, rank)]
     psi0 = [gauss_start(2, c["n"], BATCH["box"], c["seed"]) for c in cs]
 
     def params(c):
@@ -323,7 +331,8 @@ def batch_leg(G, dev, steps=BATCH_STEPS):
             for s, p in zip(solvers, psi0):
                 s.set_wfc(p)
             res, st = b.evolve(0, steps, **kw)
-        batched = st["point_steps"] / (st["device_ms"] * 1e-3)
+        batched, _, bsecs = replicas.job_rate(st["point_steps"], st["device_ms"] * 1e-3, dist,
+                                              dev)
         # sequential: the same solves, one gpue_evolve call each
         seq_ms, seq_pts = 0.0, 0.0
         for s, p, c in zip(solvers, psi0, cs):
@@ -336,12 +345,13 @@ def batch_leg(G, dev, steps=BATCH_STEPS):
     finally:
         for s in solvers:
             s.close()
-    return {"solves": len(cs), "steps": steps, "value": batched, "unit": UNIT,
-            "device_ms": st["device_ms"], "kernel_launches": st["kernel_launches"],
+    sequential, _, ssecs = replicas.job_rate(seq_pts, seq_ms * 1e-3, dist, dev)
+    return {"solves": BATCH["solves"], "ranks": world, "steps": steps, "value": batched,
+            "unit": UNIT, "device_ms": bsecs * 1e3, "kernel_launches": st["kernel_launches"],
             "graph_launches": st["graph_launches"],
             "stopped": sum(r["early_stop"] for r in res),
-            "sequential_value": seq_pts / (seq_ms * 1e-3), "sequential_device_ms": seq_ms,
-            "batched_over_sequential": batched / (seq_pts / (seq_ms * 1e-3)),
+            "sequential_value": sequential, "sequential_device_ms": ssecs * 1e3,
+            "batched_over_sequential": batched / sequential,
             "sample": "steps 0..%d of all 96 solves (checks every 100 steps, |dE|<1e-10 "
                       "absolute stop; none is expected to stop this early), complex64 with "
                       "FP64 reductions; sequential = the same solves through gpue_evolve one "
@@ -652,15 +662,15 @@ def main():
                 sms, sl = steady_state(G, s, WORK["total_steps"])
                 steady = {"value": pts * WORK["total_steps"] / (sms * 1e-3), "ms": sms,
                           "steps": WORK["total_steps"], "launches": sl}
-        if dist is not None:
-            t = torch.tensor([ms], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = replicas.max_over_ranks(ms, dist, dev)
         res[name] = dict(ms=ms, launches=launches, clocks=clocks, steady=steady)
 
     tsteps = args.steps * STEPS_PER_BENCH_STEP
     v32 = world * pts * tsteps / (res["fp32"]["ms"] * 1e-3)
     v64 = world * pts * tsteps / (res["fp64"]["ms"] * 1e-3)
+    # legs every rank takes part in (same collectives, same order)
+    e2e = None if args.quick else e2e_leg(G, torch, psi0, dev, dist=dist)
+    batched = None if args.quick else batch_leg(G, dev, dist=dist)
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -686,14 +696,13 @@ def main():
                 "note": "achieved = 16 MiB algorithmic bytes per pass launch (read+write of "
                         "the complex64 field) / mean pass duration (4 passes per time step)"}
 
+    # rank 0 alone; the CPU baseline, serving and the 3D leg only at N = 1
     cpu = None
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and world == 1:
         cpu = cpu_oracle_rate(psi0)
-    e2e = None if args.quick else e2e_leg(G, torch, psi0, dev)
     acc = accuracy_leg(G, psi0, dev)
-    batched = None if args.quick else batch_leg(G, dev)
-    served = None if args.quick else serve_leg(G, dev)
-    large = None if args.quick else large_leg(G, dev, peak)
+    served = None if args.quick or world > 1 else serve_leg(G, dev)
+    large = None if args.quick or world > 1 else large_leg(G, dev, peak)
     line = {
         "metric": METRIC, "value": v32, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": res["fp32"]["ms"] / args.steps,
