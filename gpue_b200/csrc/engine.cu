@@ -129,16 +129,16 @@ gpue_status build_tables(gpue_ctx* c, int prec, int gstate) {
     Tables& tb = c->tab[prec];
     if (tb.built_for == gstate) return GPUE_OK;
     const gpue_params& p = c->p;
-    const size_t es = elem_size(prec);
     auto al = [](size_t b) { return ((b + 255) / 256) * 256; };
-    // per axis: [vfac][kfac] double2, [tw] storage complex, [pos][mom][vreal] double
+    // per axis: [vfac][kfac] double2, [tw] FP64 complex or FP32 hi then lo,
+    // [pos][mom][vreal] double
     size_t off = 0;
     size_t offs[3][6];
     for (int a = 0; a < 3; ++a) {
         const size_t n = c->ax[a].n;
         offs[a][0] = off; off += al(n * 16);
         offs[a][1] = off; off += al(n * 16);
-        offs[a][2] = off; off += al(n * es);
+        offs[a][2] = off; off += al(n * 16);  // FP64 twiddles, or FP32 hi then lo
         for (int k = 3; k < 6; ++k) { offs[a][k] = off; off += al(n * 8); }
     }
     if (!tb.buf) CK(cudaMalloc(&tb.buf, off));
@@ -167,8 +167,11 @@ gpue_status build_tables(gpue_ctx* c, int prec, int gstate) {
             const double twr = (double)cosl(ang), twi = (double)sinl(ang);
             if (prec == GPUE_PREC_FP32) {
                 float* tw = (float*)(h.data() + offs[a][2]);
-                tw[2 * i] = (float)twr;
-                tw[2 * i + 1] = (float)twi;
+                const float hr = (float)twr, hi = (float)twi;
+                tw[2 * i] = hr;
+                tw[2 * i + 1] = hi;
+                tw[2 * (n + i)] = (float)(twr - (double)hr);
+                tw[2 * (n + i) + 1] = (float)(twi - (double)hi);
             } else {
                 double* tw = (double*)(h.data() + offs[a][2]);
                 tw[2 * i] = twr;
@@ -824,7 +827,7 @@ size_t ctx_bytes_estimate(int dim, int n, int prec) {
     size_t b = al(N * elem_size(prec)) + al(N * 16);  // state, scratch
     b += al(kNScal * sizeof(double)) + al(cap * sizeof(double2)) +
          al(kNCtr * sizeof(unsigned)) + al(4 * sizeof(int));
-    const size_t tn = 3 * (2 * al((size_t)n * 16) + al((size_t)n * elem_size(prec)) +
+    const size_t tn = 3 * (2 * al((size_t)n * 16) + al((size_t)n * 16) +
                            3 * al((size_t)n * 8));
     return b + tn;  // one precision's operator tables
 }
@@ -833,11 +836,10 @@ size_t ctx_device_bytes(const gpue_ctx* c) {
     auto al = [](size_t b) { return ((b + 255) / 256) * 256; };
     size_t b = ctx_bytes_estimate(c->dim, c->ax[0].n, c->prec);
     if (c->psi64) b += al(c->N * 16);  // FP64 shadow
-    if (c->tab[1 - c->prec].buf) {
-        const int o = 1 - c->prec;
+    if (c->tab[1 - c->prec].buf) {  // the other precision's tables (polishing)
         for (int a = 0; a < 3; ++a) {
             const size_t n = c->ax[a].n;
-            b += 2 * al(n * 16) + al(n * elem_size(o)) + 3 * al(n * 8);
+            b += 3 * al(n * 16) + 3 * al(n * 8);
         }
     }
     if (c->vtab) b += al(c->N * 8);

@@ -31,6 +31,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
 #include <utility>
 
 #include "twiddles.h"
@@ -58,7 +59,23 @@ __device__ __forceinline__ cx<T> cconj(cx<T> a) { return {a.x, -a.y}; }
 template <typename T>
 __device__ __forceinline__ cx<T> mul_mi(cx<T> a) { return {a.y, -a.x}; }
 
-// a * W_R^m, W_R = exp(-2 pi i / R), with exact shortcuts at multiples of pi/4
+// Complex64 twiddles are carried as a pair of floats, hi + lo, equal to the
+// FP64 twiddle to about 2^-48.  A single rounded float has |W|^2 = 1 - O(1e-8)
+// on average (the rounding of cos and sin is not magnitude-neutral), which
+// repeated transforms turn into a slow systematic drift of the state; with the
+// pair the product a*W carries only the rounding of the arithmetic, which is
+// unbiased.  It costs two fused multiply-adds per real output.
+constexpr bool kSplitTwiddles = true;       // stage twiddles (per-N table)
+constexpr bool kSplitConstTwiddles = true;  // butterfly constants
+
+// a * (hi + lo)
+__device__ __forceinline__ cx<float> cmul_split(cx<float> a, cx<float> hi, cx<float> lo) {
+    const float tx = fmaf(a.x, lo.x, -a.y * lo.y);
+    const float ty = fmaf(a.x, lo.y, a.y * lo.x);
+    return {fmaf(a.x, hi.x, fmaf(-a.y, hi.y, tx)), fmaf(a.x, hi.y, fmaf(a.y, hi.x, ty))};
+}
+
+// a * W_R^m, W_R = exp(-2 pi i / R), with exact shortcuts at multiples of pi/2
 template <int R, int M, typename T>
 __device__ __forceinline__ cx<T> tw_const(cx<T> a) {
     constexpr int m = ((M % R) + R) % R;
@@ -70,6 +87,11 @@ __device__ __forceinline__ cx<T> tw_const(cx<T> a) {
         return mul_mi(a);
     } else if constexpr (4 * m == 3 * R) {
         return {-a.y, a.x};
+    } else if constexpr (kSplitConstTwiddles && std::is_same<T, float>::value) {
+        constexpr double c = tw_cos(R, m), s = -tw_sin(R, m);
+        constexpr float ch = (float)c, sh = (float)s;
+        constexpr float cl = (float)(c - (double)ch), sl = (float)(s - (double)sh);
+        return cmul_split(a, cx<float>{ch, sh}, cx<float>{cl, sl});
     } else if constexpr (8 * m == R || 8 * m == 3 * R || 8 * m == 5 * R || 8 * m == 7 * R) {
         constexpr T h = (T)0.70710678118654752440;
         constexpr double c = tw_cos(R, m);
@@ -239,8 +261,12 @@ struct LineFFT {
         static constexpr int G = N / (R * P);
         static constexpr int step = N / (Ns * R);
         static constexpr int NQ = (S > 0 && P % Ns == 0) ? 1 : G;
-        static constexpr bool HOLD = NQ * (R - 1) <= 16;
-        cx<T> w[HOLD ? NQ : 1][HOLD ? R - 1 : 1];
+        // complex64 twiddles come as hi/lo pairs (the table holds N hi values
+        // and then N lo values)
+        static constexpr bool SPLIT = kSplitTwiddles && std::is_same<T, float>::value;
+        static constexpr int WPER = SPLIT ? 2 : 1;
+        static constexpr bool HOLD = NQ * (R - 1) * WPER <= 16;
+        cx<T> w[HOLD ? NQ : 1][HOLD ? R - 1 : 1][WPER];
         const cx<T>* __restrict__ tw;
         int t;
 
@@ -252,15 +278,21 @@ struct LineFFT {
                 for (int q = 0; q < NQ; ++q) {
                     const int jm = (t + P * q) % Ns;
 #pragma unroll
-                    for (int r = 1; r < R; ++r) w[q][r - 1] = tw[jm * r * step];
+                    for (int r = 1; r < R; ++r)
+#pragma unroll
+                        for (int h = 0; h < WPER; ++h) w[q][r - 1][h] = tw[h * N + jm * r * step];
                 }
             }
         }
-        __device__ __forceinline__ cx<T> get(int q, int r) const {
+        __device__ __forceinline__ cx<T> mul(cx<T> a, int q, int r) const {
             if constexpr (HOLD) {
-                return w[NQ == 1 ? 0 : q][r - 1];
+                const int qq = NQ == 1 ? 0 : q;
+                if constexpr (SPLIT) return cmul_split(a, w[qq][r - 1][0], w[qq][r - 1][1]);
+                else return cmul(a, w[qq][r - 1][0]);
             } else {
-                return tw[((t + P * q) % Ns) * r * step];
+                const int k = ((t + P * q) % Ns) * r * step;
+                if constexpr (SPLIT) return cmul_split(a, tw[k], tw[N + k]);
+                else return cmul(a, tw[k]);
             }
         }
     };
@@ -273,7 +305,7 @@ struct LineFFT {
         for (int q = 0; q < G; ++q) {
             if constexpr (S > 0) {
 #pragma unroll
-                for (int r = 1; r < R; ++r) v[q * R + r] = cmul(v[q * R + r], w->get(q, r));
+                for (int r = 1; r < R; ++r) v[q * R + r] = w->mul(v[q * R + r], q, r);
             }
             SmallDFT<R, T>::run(&v[q * R]);
         }
