@@ -64,4 +64,6 @@ def test_cli_early_stop_and_autotune(tmp_path):
     assert "Stopping early at step" in out
     E = np.loadtxt(os.path.join(tmp_path, "energyi.dat"))
     assert 2 <= len(E) < 200
-    assert abs(E[-1] - E[-2]) < 1e-6 * E[-2]
+    # GPUE writes energyi.dat with 6 significant digits (the stream default),
+    # so the last two printed values agree to that precision
+    assert abs(E[-1] - E[-2]) <= 1.5e-5 * abs(E[-2])
