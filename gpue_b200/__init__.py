@@ -173,6 +173,7 @@ def lib():
         L.gpue_batch_last_error.restype = C.c_char_p
         L.gpue_batch_evolve.argtypes = [vp, i32, C.POINTER(BatchOpts), C.POINTER(BatchResult),
                                         C.POINTER(BatchStats)]
+        L.gpue_set_gauge_tables.argtypes = [vp, vp, vp, vp]
         L.gpue_autotune.argtypes = [vp, i32]
         L.gpue_get_plan.argtypes = [vp, i32, C.POINTER(PlanInfo)]
         L.gpue_server_create.argtypes = [C.POINTER(ServerOpts), C.POINTER(vp)]
@@ -193,7 +194,7 @@ def lib():
                      "gpue_energy", "gpue_norm", "gpue_ctx_stream", "gpue_ctx_wfc_device",
                      "gpue_load_param_text", "gpue_ast_parse", "gpue_batch_create",
                      "gpue_batch_destroy", "gpue_batch_evolve", "gpue_autotune",
-                     "gpue_get_plan"):
+                     "gpue_get_plan", "gpue_set_gauge_tables"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -343,6 +344,17 @@ class Solver:
         out = PlanInfo()
         self._ck(lib().gpue_get_plan(self._h, axis, C.byref(out)))
         return out.as_dict()
+
+    def set_gauge_tables(self, Ax=None, Ay=None, Az=None):
+        """Full-field gauge components (GPUE's -A file), x fastest."""
+        keep = [None if a is None else np.ascontiguousarray(a, dtype=np.float64).ravel()
+                for a in (Ax, Ay, Az)]
+        for a in keep:
+            if a is not None and a.size != int(np.prod(self.shape)):
+                raise ValueError("gauge table has %d points, grid has %d"
+                                 % (a.size, np.prod(self.shape)))
+        ptr = [None if a is None else a.ctypes.data for a in keep]
+        self._ck(lib().gpue_set_gauge_tables(self._h, *ptr))
 
     def load_param_text(self, text, time_mode=0, doubles=None):
         """Parameter-file fields (GPUE's -I file) from "name = expr" lines."""

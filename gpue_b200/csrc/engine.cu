@@ -869,6 +869,29 @@ gpue_status unpolish(gpue_ctx* c) {
 
 }  // namespace gpue_eng
 
+namespace gpue_eng {
+
+// Uploads full-field V and A tables (FP64, N each); the passes then use the
+// table forms (ext kernels) and, when use_a, the tabulated gauge.
+gpue_status install_fields(gpue_ctx* c, const std::vector<double>& V,
+                           const std::vector<double> (&A)[3], bool use_a) {
+    if (!c->vtab) {
+        CK(cudaMalloc(&c->vtab, c->N * sizeof(double)));
+        for (auto& t : c->atab) CK(cudaMalloc(&t, c->N * sizeof(double)));
+    }
+    CK(cudaMemcpy(c->vtab, V.data(), c->N * sizeof(double), cudaMemcpyHostToDevice));
+    for (int a = 0; a < 3; ++a) {
+        CK(cudaMemcpy(c->atab[a], A[a].data(), c->N * sizeof(double), cudaMemcpyHostToDevice));
+        bool nz_any = false;
+        for (double v : A[a]) nz_any |= (v != 0.0);
+        c->atab_nonzero[a] = nz_any;
+    }
+    c->use_atab = use_a;
+    return GPUE_OK;
+}
+
+}  // namespace gpue_eng
+
 // ================================================================= C ABI ==
 
 extern "C" {
@@ -1148,18 +1171,8 @@ gpue_status gpue_load_param_text(gpue_ctx* c, const char* text, int32_t time_mod
                                    (A[0][g] * A[0][g] + A[1][g] * A[1][g] + A[2][g] * A[2][g]));
         }
     }
-    if (!c->vtab) {
-        CK(cudaMalloc(&c->vtab, c->N * sizeof(double)));
-        for (auto& t : c->atab) CK(cudaMalloc(&t, c->N * sizeof(double)));
-    }
-    CK(cudaMemcpy(c->vtab, V.data(), c->N * sizeof(double), cudaMemcpyHostToDevice));
-    for (int a = 0; a < 3; ++a) {
-        CK(cudaMemcpy(c->atab[a], A[a].data(), c->N * sizeof(double), cudaMemcpyHostToDevice));
-        bool nz_any = false;
-        for (double v : A[a]) nz_any |= (v != 0.0);
-        c->atab_nonzero[a] = nz_any;
-    }
-    c->use_atab = any_a;
+    gpue_status st = install_fields(c, V, A, any_a);
+    if (st) return st;
     // time-dependent expressions: evolve()'s *_time branches
     std::vector<AstInstr> progs;
     const char* pn[5] = {"V", "k", "Ax", "Ay", "Az"};
@@ -1183,6 +1196,40 @@ gpue_status gpue_load_param_text(gpue_ctx* c, const char* text, int32_t time_mod
         CK(cudaMemcpy(c->progs, progs.data(), progs.size() * sizeof(AstInstr),
                       cudaMemcpyHostToDevice));
     }
+    c->ext = true;
+    destroy_graphs(c);
+    return GPUE_OK;
+}
+
+gpue_status gpue_set_gauge_tables(gpue_ctx* c, const double* Ax, const double* Ay,
+                                  const double* Az) {
+    if (!c || (!Ax && !Ay && !Az)) return GPUE_ERR_INVALID_ARG;
+    CK(cudaSetDevice(c->device));
+    const gpue_params& p = c->p;
+    const int nx = c->ax[0].n, ny = c->ax[1].n;
+    std::vector<double> V(c->N), A[3];
+    const double* src[3] = {Ax, Ay, c->dim == 3 ? Az : nullptr};
+    for (int a = 0; a < 3; ++a) {
+        A[a].assign(c->N, 0.0);
+        if (src[a]) std::copy(src[a], src[a] + c->N, A[a].begin());
+    }
+    // kharmonic_V (src/operators.cu:994-1008) with the tabulated A
+    for (long g = 0; g < c->N; ++g) {
+        const int i = (int)(g % nx), j = (int)((g / nx) % ny), k = (int)(g / ((long)nx * ny));
+        const double vx = p.omegaX * (c->ax[0].x[i] + p.x0_shift);
+        const double vy = p.gammaY * p.omegaY * (c->ax[1].x[j] + p.y0_shift);
+        const double vz = (c->dim == 3 ? p.omegaZ : 0.0) *
+                          (c->ax[2].x[k] + (c->dim == 3 ? p.z0_shift : 0.0));
+        V[g] = 0.5 * p.mass * ((vx * vx + vy * vy + vz * vz) +
+                               (A[0][g] * A[0][g] + A[1][g] * A[1][g] + A[2][g] * A[2][g]));
+    }
+    gpue_status st = install_fields(c, V, A, true);
+    if (st) return st;
+    for (int k = 0; k < 5; ++k) {
+        c->prog_off[k] = -1;
+        c->prog_len[k] = 0;
+    }
+    c->time_dep = false;
     c->ext = true;
     destroy_graphs(c);
     return GPUE_OK;

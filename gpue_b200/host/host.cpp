@@ -71,6 +71,24 @@ gpue_ctx* ensure_ctx(Grid& par) {
                                    (int32_t)names.size()),
               c, "parameter file");
     }
+    if (par.Afn == "file") {
+        // file_A (src/operators.cu:259-270): whitespace-separated values times omega
+        const size_t n = (size_t)par.ival("xDim") * par.ival("yDim") * par.ival("zDim");
+        std::vector<double> A[3];
+        const char* keys[3] = {"Axfile", "Ayfile", "Azfile"};
+        for (int a = 0; a < (par.ival("dimnum") == 3 ? 3 : 2); ++a) {
+            std::ifstream in(par.sval(keys[a]));
+            double v;
+            while (in >> v) A[a].push_back(par.dval("omega") * v);
+            if (A[a].size() != n)
+                throw std::runtime_error(par.sval(keys[a]) + " has " +
+                                         std::to_string(A[a].size()) + " values, the grid " +
+                                         std::to_string(n));
+        }
+        check(gpue_set_gauge_tables(c, A[0].data(), A[1].data(),
+                                    A[2].empty() ? nullptr : A[2].data()),
+              c, "gauge from file");
+    }
     if (par.bval("autotune")) check(gpue_autotune(c, 0), c, "gpue_autotune");
     return c;
 }
@@ -260,6 +278,11 @@ Grid parse_args(int argc, char** argv) {
         par.store("infile", filecheck(data_dir + "wfc_load"));
         par.store("infilei", filecheck(data_dir + "wfci_load"));
     }
+    if (par.Afn == "file") {  // src/parser.cu:478-487
+        par.store("Axfile", filecheck(data_dir + "Axgauge"));
+        par.store("Ayfile", filecheck(data_dir + "Aygauge"));
+        if (par.ival("dimnum") == 3) par.store("Azfile", filecheck(data_dir + "Azgauge"));
+    }
     return par;
 }
 
@@ -269,9 +292,10 @@ void init(Grid& par) {
     const int dimnum = par.ival("dimnum");
     if (dimnum != 2 && dimnum != 3)
         throw std::runtime_error("this build runs 2D and 3D grids (-c 2 or -c 3)");
-    if (par.Afn != "rotation" && par.Afn != "constant")
+    if (par.Afn != "rotation" && par.Afn != "constant" && par.Afn != "file")
         throw std::runtime_error("gauge field '" + par.Afn +
-                                 "' is not built; use rotation, constant or a parameter file");
+                                 "' is not built; use rotation, constant, file or a "
+                                 "parameter file");
     if (par.Vfn != "2d" && par.Vfn != "3d")
         throw std::runtime_error("potential '" + par.Vfn +
                                  "' is not built; use the harmonic trap or a parameter file");

@@ -168,6 +168,15 @@ gpue_status gpue_load_param_text(gpue_ctx* ctx, const char* text, int32_t time_m
 gpue_status gpue_ast_parse(const char* expr, const char* const* names, const double* values,
                            int32_t nvalues, void* nodes_out, int32_t cap, int32_t* count);
 
+/* GPUE's file gauge (-A file: file_A and generate_gauge, src/operators.cu:259-270,
+ * 505-520): full-field Ax, Ay, Az (host arrays of xDim*yDim*zDim doubles, x
+ * fastest, already multiplied by omega as file_A does; NULL for a zero
+ * component, Az ignored in 2D) replace the preset gauge.  V becomes the
+ * harmonic trap plus m|A|^2/2 (kharmonic_V, src/operators.cu:994-1008) over
+ * the full grid, and the gauge passes apply exp(-i A p dt) per point. */
+gpue_status gpue_set_gauge_tables(gpue_ctx* ctx, const double* Ax, const double* Ay,
+                                  const double* Az);
+
 /* Device pointer of the resident wavefunction and its dtype (GPUE_C128/C64). */
 gpue_status gpue_ctx_wfc_device(gpue_ctx* ctx, void** psi, int32_t* dtype);
 

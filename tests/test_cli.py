@@ -99,7 +99,8 @@ def test_read_wfc_files(tmp_path):
 
 @pytest.mark.parametrize("args,msg", [
     (["-r"], "wfc_load"),                       # -r without the input files
-    (["-A", "file"], "gauge field"),
+    (["-A", "file"], "Axgauge"),                # -A file without the gauge files
+    (["-A", "ring"], "gauge field"),
     (["-v", "torus"], "potential"),
     (["-c", 1], "2D and 3D"),
     (["--no-such-option"], "unknown option"),
