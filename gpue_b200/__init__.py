@@ -100,6 +100,15 @@ class PlanInfo(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Observables(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("norm", "energy", "e_kinetic", "e_potential",
+                                          "e_interaction", "e_rotation", "x", "y", "z",
+                                          "r2", "q", "lz")] + [("reserved", C.c_double * 4)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
 class ServerOpts(C.Structure):
     _fields_ = [("device", C.c_int32), ("precision", C.c_int32),
                 ("hbm_budget_bytes", C.c_int64), ("check_steps", C.c_int32),
@@ -159,6 +168,7 @@ def lib():
         L.gpue_evolve.argtypes = [vp, i32, i32, C.POINTER(EvolveOpts), C.POINTER(EvolveResult)]
         L.gpue_energy.argtypes = [vp, C.POINTER(C.c_double)]
         L.gpue_norm.argtypes = [vp, C.POINTER(C.c_double)]
+        L.gpue_observables_get.argtypes = [vp, C.POINTER(Observables)]
         L.gpue_ctx_stream.argtypes = [vp, C.POINTER(vp)]
         L.gpue_ctx_wfc_device.argtypes = [vp, C.POINTER(vp), C.POINTER(i32)]
         L.gpue_norm_noalloc.argtypes = [vp, i32, C.c_int64, C.c_double, vp, vp]
@@ -194,7 +204,7 @@ def lib():
                      "gpue_energy", "gpue_norm", "gpue_ctx_stream", "gpue_ctx_wfc_device",
                      "gpue_load_param_text", "gpue_ast_parse", "gpue_batch_create",
                      "gpue_batch_destroy", "gpue_batch_evolve", "gpue_autotune",
-                     "gpue_get_plan", "gpue_set_gauge_tables"):
+                     "gpue_get_plan", "gpue_set_gauge_tables", "gpue_observables_get"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -324,6 +334,13 @@ class Solver:
         e = C.c_double()
         self._ck(lib().gpue_norm(self._h, C.byref(e)))
         return e.value
+
+    def observables(self):
+        """Energy terms, trapezoid density moments and <L_z> of the current
+        state (gpue_observables_get), as a dict."""
+        o = Observables()
+        self._ck(lib().gpue_observables_get(self._h, C.byref(o)))
+        return o.as_dict()
 
     def stream(self):
         s = C.c_void_p()

@@ -32,6 +32,44 @@ struct EnergyArgs {
     const double* atab[3];  // full-field A (parameter-file form), else rotation
 };
 
+// GPUE's derive() at flat index g: (psi[g+stride] - psi[g]) / d, or
+// psi[g] / d where g+stride runs past the end.  (px, py) = s*psi[g].
+template <typename T>
+__device__ __forceinline__ void dfwd(const cx<T>* psi, long N, long g, long stride, double s,
+                                     double px, double py, double d, double& ox, double& oy) {
+    if (g + stride < N) {
+        const cx<T> q = psi[g + stride];
+        ox = (s * (double)q.x - px) / d;
+        oy = (s * (double)q.y - py) / d;
+    } else {
+        ox = px / d;
+        oy = py / d;
+    }
+}
+
+// Re[conj(psi) i hbar (Ax d+x psi + Ay d+y psi [+ Az d+z psi])] at point g.
+template <typename T>
+__device__ __forceinline__ double gauge_energy(const EnergyArgs& a, const cx<T>* psi, long g,
+                                               int xi, int yi, long nxy, double s, double px,
+                                               double py) {
+    double dxr, dxi, dyr, dyi;
+    dfwd(psi, a.N, g, 1, s, px, py, a.dx, dxr, dxi);
+    dfwd(psi, a.N, g, a.nx, s, px, py, a.dy, dyr, dyi);
+    const double Ax = a.atab[0] ? a.atab[0][g] : a.ax_coef * a.pos[1][yi];
+    const double Ay = a.atab[1] ? a.atab[1][g] : a.ay_coef * a.pos[0][xi];
+    double lr = dxr * Ax + dyr * Ay;
+    double li = dxi * Ax + dyi * Ay;
+    if (a.dim == 3 && a.atab[2]) {
+        double dzr, dzi;
+        dfwd(psi, a.N, g, nxy, s, px, py, a.dz, dzr, dzi);
+        lr += dzr * a.atab[2][g];
+        li += dzi * a.atab[2][g];
+    }
+    // i*hbar*l, then Re[conj(p) * (i hbar l)]
+    const double ir = -a.hbar * li, ii = a.hbar * lr;
+    return px * ir + py * ii;
+}
+
 template <typename T>
 __device__ __forceinline__ KSum energy_real_points(const EnergyArgs& a, long g0, long gstep) {
     const cx<T>* psi = reinterpret_cast<const cx<T>*>(a.psi);
@@ -47,34 +85,7 @@ __device__ __forceinline__ KSum energy_real_points(const EnergyArgs& a, long g0,
         const double r = px * px + py * py;
         const double V = a.vtab ? a.vtab[g] : a.vreal[0][xi] + a.vreal[1][yi] + a.vreal[2][zi];
         double e = a.gpe ? r * (V + 0.5 * a.gN * r) : r * V;
-        if (a.lterm) {
-            auto dfwd = [&](long stride, double d, double& ox, double& oy) {
-                if (g + stride < a.N) {
-                    const cx<T> q = psi[g + stride];
-                    ox = (s * (double)q.x - px) / d;
-                    oy = (s * (double)q.y - py) / d;
-                } else {
-                    ox = px / d;
-                    oy = py / d;
-                }
-            };
-            double dxr, dxi, dyr, dyi;
-            dfwd(1, a.dx, dxr, dxi);
-            dfwd(a.nx, a.dy, dyr, dyi);
-            const double Ax = a.atab[0] ? a.atab[0][g] : a.ax_coef * a.pos[1][yi];
-            const double Ay = a.atab[1] ? a.atab[1][g] : a.ay_coef * a.pos[0][xi];
-            double lr = dxr * Ax + dyr * Ay;
-            double li = dxi * Ax + dyi * Ay;
-            if (a.dim == 3 && a.atab[2]) {
-                double dzr, dzi;
-                dfwd(nxy, a.dz, dzr, dzi);
-                lr += dzr * a.atab[2][g];
-                li += dzi * a.atab[2][g];
-            }
-            // i*hbar*l, then Re[conj(p) * (i hbar l)]
-            const double ir = -a.hbar * li, ii = a.hbar * lr;
-            e += px * ir + py * ii;
-        }
+        if (a.lterm) e += gauge_energy<T>(a, psi, g, xi, yi, nxy, s, px, py);
         acc.add(e);
     }
     return acc;
@@ -100,6 +111,109 @@ __global__ void __launch_bounds__(256) k_energy_real_batch(const EnergyArgs* __r
     const EnergyArgs& a = args[s];
     KSum acc = energy_real_points<T>(a, (long)b * blockDim.x + threadIdx.x, (long)per * blockDim.x);
     grid_reduce_finish(acc, scratch, a.red, per, b);
+}
+
+// Observables of one state (gpue_observables_get): the real-space energy
+// terms, trapezoid density moments and <L_z>, reduced in FP64 per quantity.
+// Each CTA writes kObsN compensated partials ([q][gridDim.x]); the last CTA to
+// arrive sums every quantity in CTA order (deterministic) into out[q].
+enum ObsQ {
+    kObsNorm, kObsPot, kObsInt, kObsRot, kObsX, kObsY, kObsZ, kObsR2, kObsQ, kObsLz, kObsN
+};
+
+struct ObsArgs {
+    EnergyArgs e;
+    double2* partials;  // [kObsN][gridDim.x]
+    unsigned* counter;  // zero between launches; reset by the last CTA
+    double* out;        // [kObsN]
+};
+
+__device__ __forceinline__ double trapz_w(int i, int n) {
+    return (n > 1 && (i == 0 || i == n - 1)) ? 0.5 : 1.0;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_observables(const ObsArgs o) {
+    __shared__ double scratch[kObsN][16];
+    __shared__ unsigned s_last;
+    const EnergyArgs& a = o.e;
+    const cx<T>* psi = reinterpret_cast<const cx<T>*>(a.psi);
+    const double s = a.scale ? *a.scale : 1.0;
+    const long nxy = (long)a.nx * a.ny;
+    KSum acc[kObsN];
+#pragma unroll
+    for (int q = 0; q < kObsN; ++q) acc[q] = KSum{0.0, 0.0};
+    for (long g = (long)blockIdx.x * blockDim.x + threadIdx.x; g < a.N;
+         g += (long)gridDim.x * blockDim.x) {
+        const int xi = (int)(g % a.nx);
+        const int yi = (int)((g / a.nx) % a.ny);
+        const int zi = (int)(g / nxy);
+        const cx<T> pv = psi[g];
+        const double px = s * (double)pv.x, py = s * (double)pv.y;
+        const double r = px * px + py * py;
+        const double V = a.vtab ? a.vtab[g] : a.vreal[0][xi] + a.vreal[1][yi] + a.vreal[2][zi];
+        acc[kObsNorm].add(r);
+        acc[kObsPot].add(r * V);
+        if (a.gpe) acc[kObsInt].add(0.5 * a.gN * r * r);
+        if (a.lterm) acc[kObsRot].add(gauge_energy<T>(a, psi, g, xi, yi, nxy, s, px, py));
+        const double X = a.pos[0][xi];
+        const double Y = a.dim > 1 ? a.pos[1][yi] : 0.0;
+        const double Z = a.dim > 2 ? a.pos[2][zi] : 0.0;
+        const double wr = r * trapz_w(xi, a.nx) * trapz_w(yi, a.ny) * trapz_w(zi, a.nz);
+        acc[kObsX].add(wr * X);
+        acc[kObsY].add(wr * Y);
+        acc[kObsZ].add(wr * Z);
+        acc[kObsR2].add(wr * (X * X + Y * Y));
+        acc[kObsQ].add(wr * (X * X - Y * Y));
+        if (a.dim > 1) {
+            // -i hbar (x d+y - y d+x) psi, then Re[conj(p) * that]
+            double dxr, dxi, dyr, dyi;
+            dfwd(psi, a.N, g, 1, s, px, py, a.dx, dxr, dxi);
+            dfwd(psi, a.N, g, a.nx, s, px, py, a.dy, dyr, dyi);
+            const double Dr = X * dyr - Y * dxr, Di = X * dyi - Y * dxi;
+            acc[kObsLz].add(a.hbar * (px * Di - py * Dr));
+        }
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int q = 0; q < kObsN; ++q) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const double os = __shfl_down_sync(0xffffffffu, acc[q].s, off);
+            const double oc = __shfl_down_sync(0xffffffffu, acc[q].c, off);
+            acc[q].merge(os, oc);
+        }
+        if (lane == 0) {
+            scratch[q][2 * w] = acc[q].s;
+            scratch[q][2 * w + 1] = acc[q].c;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < kObsN) {
+        const int q = threadIdx.x;
+        KSum t{scratch[q][0], scratch[q][1]};
+        for (int i = 1; i < nw; ++i) t.merge(scratch[q][2 * i], scratch[q][2 * i + 1]);
+        o.partials[(long)q * gridDim.x + blockIdx.x] = make_double2(t.s, t.c);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned prev = atomicAdd(o.counter, 1u);
+        s_last = (prev == gridDim.x - 1) ? 1u : 0u;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (threadIdx.x < kObsN) {
+        const int q = threadIdx.x;
+        KSum t{0.0, 0.0};
+        for (unsigned i = 0; i < gridDim.x; ++i) {
+            const double2 p = __ldcg(o.partials + (long)q * gridDim.x + i);
+            t.merge(p.x, p.y);
+        }
+        o.out[q] = t.s + t.c;
+    }
+    if (threadIdx.x == 0) *o.counter = 0u;
 }
 
 // Energy check of batched solves, one block.  flags[2] counts a solve's

@@ -1086,6 +1086,53 @@ gpue_status gpue_energy(gpue_ctx* c, double* E) {
     return read_energy(c, E);
 }
 
+gpue_status gpue_observables_get(gpue_ctx* c, gpue_observables* o) {
+    if (!c || !o) return GPUE_ERR_INVALID_ARG;
+    if (!c->have_wfc) return fail(c, GPUE_ERR_STATE, "no wavefunction set");
+    CK(cudaSetDevice(c->device));
+    const int sp = c->polished ? GPUE_PREC_FP64 : c->prec;
+    const int gs = c->tab[sp].built_for < 0 ? 0 : c->tab[sp].built_for;
+    gpue_status st = build_tables(c, sp, gs);
+    if (st) return st;
+    bool pdl = false;
+    for (auto& lp : energy_passes(c, c->pending_scale)) {
+        st = launch_pass(c, sp, lp, gs, pdl);
+        if (st) return st;
+        pdl = true;
+    }
+    ObsArgs oa;
+    std::memset(&oa, 0, sizeof oa);
+    oa.e = energy_args(c, sp, c->pending_scale);
+    double2* aux = c->partials + (c->partials_cap - kAuxPartials);
+    const int blocks = (int)std::min<long>(c->sms * 2, (kAuxPartials - kObsN) / kObsN);
+    oa.partials = aux;
+    oa.counter = c->counters + kCtrMisc;
+    oa.out = reinterpret_cast<double*>(aux + (long)kObsN * blocks);
+    if (sp == GPUE_PREC_FP32) k_observables<float><<<blocks, 256, 0, c->stream>>>(oa);
+    else k_observables<double><<<blocks, 256, 0, c->stream>>>(oa);
+    c->launches++;
+    CK(cudaGetLastError());
+    double h[kObsN], ekin;
+    CK(cudaMemcpyAsync(h, oa.out, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(&ekin, c->scal + kEkin, sizeof ekin, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::memset(o, 0, sizeof *o);
+    const double dV = c->dV;
+    o->norm = h[kObsNorm] * dV;
+    o->e_kinetic = ekin / (double)c->N * dV;
+    o->e_potential = h[kObsPot] * dV;
+    o->e_interaction = h[kObsInt] * dV;
+    o->e_rotation = h[kObsRot] * dV;
+    o->energy = o->e_kinetic + o->e_potential + o->e_interaction + o->e_rotation;
+    o->x = h[kObsX] * dV;
+    o->y = h[kObsY] * dV;
+    o->z = h[kObsZ] * dV;
+    o->r2 = h[kObsR2] * dV;
+    o->q = h[kObsQ] * dV;
+    o->lz = h[kObsLz] * dV;
+    return GPUE_OK;
+}
+
 gpue_status gpue_norm(gpue_ctx* c, double* out) {
     if (!c || !out) return GPUE_ERR_INVALID_ARG;
     CK(cudaSetDevice(c->device));

@@ -16,6 +16,9 @@
  *   gpue_evolve          evolve(par, numSteps, gstate, buffer)
  *                        include/evolution.h:54-57, src/evolution.cu:260-908
  *   gpue_energy          energy_calc(par, wfc)  src/split_op.cu:208-375
+ *   gpue_observables_get the energy terms and moments computed from written
+ *                        wavefunctions by julia/calc_energy.jl:32-66 and
+ *                        py/en.py:44-66
  *   gpue_last_error      cudaHandleError/cudaCheckError/cufftHandleError
  *                        (src/split_op.cu:40-59) report-and-exit replaced by
  *                        status codes plus a message
@@ -143,6 +146,40 @@ gpue_status gpue_energy(gpue_ctx* ctx, double* energy);
 
 /* sum |psi|^2 dV of the current state. */
 gpue_status gpue_norm(gpue_ctx* ctx, double* norm);
+
+/* Observables of the current state, one real-space pass plus the kinetic
+ * passes of energy_calc.  Replaces the post-processing GPUE does on written
+ * wavefunctions:
+ *   - the energy split into its terms as julia/calc_energy.jl:32-66 prints
+ *     them (kinetic, potential, internal, angular-momentum), with the terms
+ *     formed exactly as energy_calc (src/split_op.cu:208-375) forms them:
+ *     plain sums times dV, V including the m|A|^2/2 gauge term, and the
+ *     gauge term through GPUE's forward difference derive()
+ *     (src/kernels.cu:58-71, no periodic wrap);  e_kinetic + e_potential +
+ *     e_interaction + e_rotation = energy = gpue_energy() up to rounding;
+ *   - the density moments of py/en.py:44-50 (expectValueR with X, Y, R =
+ *     X^2+Y^2 and Q = X^2-Y^2), integrated with np.trapz's weights (1/2 on
+ *     the first and last point of each axis) times dV; x is the contiguous
+ *     axis;
+ *   - <L_z> = sum Re[conj(psi) (-i hbar)(x d+y psi - y d+x psi)] dV with the
+ *     same forward differences, so e_rotation = -omega*omegaY * lz for the
+ *     rotation gauge with omegaX = omegaY.
+ * None of the values is divided by the norm. */
+typedef struct gpue_observables {
+    double norm;            /* sum |psi|^2 dV */
+    double energy;          /* sum of the four terms below */
+    double e_kinetic;       /* sum_k K |psi_k|^2 / N dV */
+    double e_potential;     /* sum V |psi|^2 dV */
+    double e_interaction;   /* sum gN/2 |psi|^4 dV (0 without the nonlinearity) */
+    double e_rotation;      /* sum Re[conj(psi) i hbar A.d+ psi] dV (corotating only) */
+    double x, y, z;         /* trapezoid <x>, <y>, <z> (0 for absent axes) */
+    double r2;              /* trapezoid <x^2 + y^2> */
+    double q;               /* trapezoid <x^2 - y^2> */
+    double lz;              /* <L_z> */
+    double reserved[4];
+} gpue_observables;
+
+gpue_status gpue_observables_get(gpue_ctx* ctx, gpue_observables* out);
 
 /* The context's cudaStream_t (as void*) for callers that time or order work. */
 gpue_status gpue_ctx_stream(gpue_ctx* ctx, void** stream);

@@ -63,6 +63,8 @@ def test_invalid_arguments_fail_without_touching_the_device():
     assert L.gpue_ctx_create(ctypes.byref(bad), ctypes.byref(h)) == 2
     assert L.gpue_evolve(None, 1, 0, None, None) == 1
     assert L.gpue_set_operators(None, 0) == 1
+    obs = G.Observables()
+    assert L.gpue_observables_get(None, ctypes.byref(obs)) == 1
     # batches: argument checks come before any device call
     out = ctypes.c_void_p()
     assert L.gpue_batch_create(None, 1, ctypes.byref(out)) == 1
