@@ -109,6 +109,15 @@ class Observables(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
+class Vortex(C.Structure):
+    _fields_ = [("i", C.c_int32), ("j", C.c_int32), ("marker", C.c_int32),
+                ("winding", C.c_int32)]
+
+
+VORTEX_DTYPE = np.dtype([("i", np.int32), ("j", np.int32), ("marker", np.int32),
+                         ("winding", np.int32)])
+
+
 class ServerOpts(C.Structure):
     _fields_ = [("device", C.c_int32), ("precision", C.c_int32),
                 ("hbm_budget_bytes", C.c_int64), ("check_steps", C.c_int32),
@@ -169,6 +178,7 @@ def lib():
         L.gpue_energy.argtypes = [vp, C.POINTER(C.c_double)]
         L.gpue_norm.argtypes = [vp, C.POINTER(C.c_double)]
         L.gpue_observables_get.argtypes = [vp, C.POINTER(Observables)]
+        L.gpue_find_vortices.argtypes = [vp, C.c_double, vp, i32, vp, i32, C.POINTER(i32)]
         L.gpue_ctx_stream.argtypes = [vp, C.POINTER(vp)]
         L.gpue_ctx_wfc_device.argtypes = [vp, C.POINTER(vp), C.POINTER(i32)]
         L.gpue_norm_noalloc.argtypes = [vp, i32, C.c_int64, C.c_double, vp, vp]
@@ -204,7 +214,8 @@ def lib():
                      "gpue_energy", "gpue_norm", "gpue_ctx_stream", "gpue_ctx_wfc_device",
                      "gpue_load_param_text", "gpue_ast_parse", "gpue_batch_create",
                      "gpue_batch_destroy", "gpue_batch_evolve", "gpue_autotune",
-                     "gpue_get_plan", "gpue_set_gauge_tables", "gpue_observables_get"):
+                     "gpue_get_plan", "gpue_set_gauge_tables", "gpue_observables_get",
+                     "gpue_find_vortices"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -334,6 +345,20 @@ class Solver:
         e = C.c_double()
         self._ck(lib().gpue_norm(self._h, C.byref(e)))
         return e.value
+
+    def find_vortices(self, radius, cap=None):
+        """Tracker::findVortex on the resident 2D state (gpue_find_vortices):
+        (marker int32 (n, n), list of marks as a VORTEX_DTYPE array, found)."""
+        n = self.params.xDim
+        marker = np.zeros((n, n), np.int32)
+        cap = n * n // 2 + 1 if cap is None else int(cap)
+        lst = np.zeros(max(cap, 1), VORTEX_DTYPE)
+        found = C.c_int32()
+        vp = C.c_void_p
+        self._ck(lib().gpue_find_vortices(self._h, float(radius), marker.ctypes.data_as(vp),
+                                          MEM_HOST, lst.ctypes.data_as(vp) if cap else None,
+                                          cap, C.byref(found)))
+        return marker, lst[:min(found.value, cap)], found.value
 
     def observables(self):
         """Energy terms, trapezoid density moments and <L_z> of the current

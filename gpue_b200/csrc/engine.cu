@@ -1000,6 +1000,7 @@ gpue_status gpue_ctx_destroy(gpue_ctx* c) {
     for (auto t : c->atab)
         if (t) cudaFree(t);
     if (c->progs) cudaFree(c->progs);
+    if (c->vtx_ws) cudaFree(c->vtx_ws);
     cudaFree(c->scratch);
     cudaFree(c->scal);
     cudaFree(c->partials);

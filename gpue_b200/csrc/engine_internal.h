@@ -110,6 +110,8 @@ struct gpue_ctx {
     int prog_off[5] = {-1, -1, -1, -1, -1};  // V, k, Ax, Ay, Az
     int prog_len[5] = {};
     bool time_dep = false;     // some factor is evaluated per step
+    void* vtx_ws = nullptr;    // gpue_find_vortices workspace (allocated on first use)
+    size_t vtx_ws_bytes = 0;
 };
 
 namespace gpue_eng {

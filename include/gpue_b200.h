@@ -19,6 +19,7 @@
  *   gpue_observables_get the energy terms and moments computed from written
  *                        wavefunctions by julia/calc_energy.jl:32-66 and
  *                        py/en.py:44-66
+ *   gpue_find_vortices   Tracker::findVortex  src/tracker.cu:102-166
  *   gpue_last_error      cudaHandleError/cudaCheckError/cufftHandleError
  *                        (src/split_op.cu:40-59) report-and-exit replaced by
  *                        status codes plus a message
@@ -180,6 +181,34 @@ typedef struct gpue_observables {
 } gpue_observables;
 
 gpue_status gpue_observables_get(gpue_ctx* ctx, gpue_observables* out);
+
+/* 2D vortex finder: Tracker::findVortex (src/tracker.cu:102-166), which GPUE
+ * runs on a host copy of the state at print steps in real time
+ * (src/evolution.cu:430, 483-486), here on the resident state.  Plaquette
+ * (i, j), i the row (y index) and j the column (x index), i, j < xDim-1, is
+ * examined when sqrt(x_i^2 + x_j^2) < radius (GPUE's x grid on both axes) by
+ * summing the wrapped phase steps around (i,j) -> (i+1,j) -> (i+1,j+1) ->
+ * (i,j+1); a sum of magnitude >= 1.9 pi marks it with |lround(sum / 2 pi)|,
+ * except that the in-radius plaquette visited right after a marked one (rows
+ * in order, columns in order within a row) is never marked, as findVortex's
+ * cond_x/cond_y counters have it.
+ *   marker  xDim*yDim int32 in GPUE's layout (index i*xDim + j), zero except
+ *           at marks; may be NULL; mem = GPUE_MEM_HOST or GPUE_MEM_DEVICE
+ *           says where marker and list live;
+ *   list    the first min(found, cap) marks in visiting order with the
+ *           signed winding (x + i y around a point carries +1); may be NULL;
+ *   found   number of marks (findVortex's return value).
+ * 2D contexts only (GPUE_ERR_UNSUPPORTED otherwise).  The first call on a
+ * context allocates a device workspace of about 13 bytes per grid point,
+ * kept until gpue_ctx_destroy. */
+typedef struct gpue_vortex {
+    int32_t i, j;       /* row (y index), column (x index) of the plaquette corner */
+    int32_t marker;     /* the value findVortex stores there */
+    int32_t winding;    /* signed lround(sum / 2 pi) */
+} gpue_vortex;
+
+gpue_status gpue_find_vortices(gpue_ctx* ctx, double radius, int32_t* marker, int32_t mem,
+                               gpue_vortex* list, int32_t cap, int32_t* found);
 
 /* The context's cudaStream_t (as void*) for callers that time or order work. */
 gpue_status gpue_ctx_stream(gpue_ctx* ctx, void** stream);

@@ -20,6 +20,7 @@
 //   renormalisation          src/split_op.cu:83-129
 //   energy                   src/split_op.cu:208-375, derive src/kernels.cu:58-71
 //   AST evaluation           src/dynamic.cu:527-603
+//   2D vortex finder         src/tracker.cu:102-166 (Tracker::findVortex)
 //
 // The DFT is this file's own mixed-radix Stockham transform (radices 2,3,4,5
 // and a direct DFT for other primes); FFTW is not available.
@@ -638,3 +639,65 @@ void orc_std_wfc(int nx, int ny, int nz, const double* x, const double* y, const
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------ vortices --
+//
+// Tracker::findVortex (src/tracker.cu:102-166), restated.  The plaquettes
+// (i, j), i < n-1 the slow (row) index and j < n-1 the contiguous one, are
+// visited row by row; those with sqrt(x[i]^2 + x[j]^2) < radius (the x array
+// serves both axes: GPUE's grids are square) sum the wrapped phase steps
+// arg(w_a) - arg(w_b) around (i,j) -> (i+1,j) -> (i+1,j+1) -> (i,j+1) -> (i,j),
+// each phase taken of (w_a conj(w_b)) / |w_b|^2 * |w_b|/|w_a| with atan2 and
+// moved from (-inf, -pi] up by 2 pi.  A sum >= 1.9 pi or <= -1.9 pi marks the
+// plaquette with |lround(sum / 2 pi)| (findVortex stores -lround for negative
+// sums) unless the previous in-radius plaquette in visiting order was marked:
+// the two counters findVortex sets to 2 on a mark and decrements after every
+// in-radius plaquette skip exactly the next one.  marker (n*n ints) must be
+// zero on entry; winding, if not null, receives the signed lround at marked
+// plaquettes.  Returns the number of marks.
+namespace {
+struct c2 {
+    double x, y;
+};
+c2 cdiv_scaled(c2 a, c2 b) {
+    // complexScale(complexDiv(a, b), |b| / |a|) (src/minions.cu:62-93)
+    const c2 cb{b.x, -b.y};
+    const c2 m{a.x * cb.x - a.y * cb.y, a.x * cb.y + a.y * cb.x};
+    const double inv = 1.0 / (b.x * b.x + b.y * b.y);
+    const c2 q{m.x * inv, m.y * inv};
+    const double r = std::sqrt(b.x * b.x + b.y * b.y) / std::sqrt(a.x * a.x + a.y * a.y);
+    return c2{q.x * r, q.y * r};
+}
+}  // namespace
+
+extern "C" int orc_find_vortex(const double* wfc, int n, const double* x, double radius,
+                               int* marker, int* winding) {
+    const double PI = 3.141592653589793;
+    const c2* w = reinterpret_cast<const c2*>(wfc);
+    int found = 0;
+    bool skip_next = false;  // the previous in-radius plaquette was marked
+    for (int i = 0; i < n - 1; ++i) {
+        for (int j = 0; j < n - 1; ++j) {
+            if (!(std::sqrt(x[i] * x[i] + x[j] * x[j]) < radius)) continue;
+            const c2 corner[4] = {w[i * n + j], w[(i + 1) * n + j], w[(i + 1) * n + j + 1],
+                                  w[i * n + j + 1]};
+            double d[4];
+            for (int k = 0; k < 4; ++k) {
+                const c2 g = cdiv_scaled(corner[k], corner[(k + 1) & 3]);
+                d[k] = std::atan2(g.y, g.x);
+                if (d[k] <= -PI) d[k] += 2 * PI;
+            }
+            const double sum = d[0] + d[1] + d[2] + d[3];
+            const bool mark = !skip_next && (sum >= 1.9 * PI || sum <= -1.9 * PI);
+            if (mark) {
+                const long r = std::lround(sum / (2 * PI));
+                marker[i * n + j] = (int)(r < 0 ? -r : r);
+                if (winding) winding[i * n + j] = (int)r;
+                ++found;
+            }
+            skip_next = mark;
+        }
+    }
+    return found;
+}
+

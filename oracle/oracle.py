@@ -58,6 +58,9 @@ def lib():
         L.orc_fields.argtypes = ([C.c_int] * 4 + [dp] * 6 + [C.c_double] * 10 + [C.c_int]
                                  + [dp] * 5)
         L.orc_ast_eval.argtypes = [C.POINTER(Node)] + [C.c_double] * 4
+        ip = C.POINTER(C.c_int)
+        L.orc_find_vortex.argtypes = [dp, C.c_int, dp, C.c_double, ip, ip]
+        L.orc_find_vortex.restype = C.c_int
         L.orc_ast_eval.restype = C.c_double
         L.orc_std_wfc.argtypes = [C.c_int] * 3 + [dp] * 3 + [C.c_double] * 5 + [dp]
         _LIB = L
@@ -154,3 +157,20 @@ class Problem:
         a = np.ascontiguousarray(psi, dtype=np.complex128)
         return lib().orc_energy(C.byref(self.cfg), _p(self.V), _p(self.K), _p(self.Ax),
                                 _p(self.Ay), _p(self.Az), _p(a.view(np.float64)))
+
+
+def find_vortex(psi, x, radius):
+    """Tracker::findVortex (src/tracker.cu:102-166) on a complex128 (n, n)
+    state [y, x] with grid x: (marker, winding, found), marker and winding
+    int32 (n, n) arrays (winding: signed lround at the marks)."""
+    a = np.ascontiguousarray(psi, dtype=np.complex128)
+    n = a.shape[0]
+    assert a.shape == (n, n)
+    xs = np.ascontiguousarray(x, dtype=np.float64)
+    marker = np.zeros((n, n), np.int32)
+    winding = np.zeros((n, n), np.int32)
+    ip = C.POINTER(C.c_int)
+    found = lib().orc_find_vortex(_p(a.view(np.float64)), n, _p(xs), radius,
+                                  marker.ctypes.data_as(ip), winding.ctypes.data_as(ip))
+    return marker, winding, found
+

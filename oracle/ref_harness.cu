@@ -20,6 +20,12 @@
 // Writes prefix_imag.bin / prefix_real.bin (complex128, x fastest, hbar=m=1
 // units) and prefix_imag.txt / prefix_real.txt ("energy <E>" and
 // "last_check_energy <E>", plus "evolve_s <seconds>" of the evolve() call).
+//
+//   gpue_ref_harness mode=vortex n=128 box=8 radius=5 psi0=in.bin out=prefix
+// runs only GPUE's host-side Tracker::findVortex (src/tracker.cu:102-166) on
+// the n x n complex128 state in psi0 with GPUE's x grid, and writes the marker
+// array (int32, n*n) to prefix_vortex.bin and "found <count>" to
+// prefix_vortex.txt.  This mode makes no CUDA call and needs no GPU.
 
 #include <chrono>
 #include <cmath>
@@ -35,6 +41,7 @@
 #include "init.h"
 #include "parser.h"
 #include "split_op.h"
+#include "tracker.h"
 
 namespace {
 
@@ -74,6 +81,36 @@ void dump(Grid& par, const std::string& path, int gsize, double L, int dim, doub
     fclose(t);
 }
 
+int vortex_mode() {
+    const int n = geti("n", 64);
+    const double xMax = getd("box", 10);
+    std::vector<double2> wfc((size_t)n * n);
+    FILE* f = fopen(get("psi0", "psi0.bin").c_str(), "rb");
+    if (!f || fread(wfc.data(), sizeof(double2), wfc.size(), f) != wfc.size()) {
+        fprintf(stderr, "cannot read psi0\n");
+        return 2;
+    }
+    fclose(f);
+    // generate_p_space's x (src/operators.cu:336-343)
+    std::vector<double> x(n);
+    const double dx = xMax / (n >> 1);
+    for (int i = 0; i < n / 2; ++i) {
+        x[i] = -xMax + i * dx;
+        x[i + n / 2] = i * dx;
+    }
+    std::vector<int> marker((size_t)n * n, 0);
+    const int found = Tracker::findVortex(marker.data(), wfc.data(), getd("radius", 1.0), n,
+                                          x.data(), 0);
+    const std::string out = get("out", "ref");
+    FILE* b = fopen((out + "_vortex.bin").c_str(), "wb");
+    fwrite(marker.data(), sizeof(int), marker.size(), b);
+    fclose(b);
+    FILE* t = fopen((out + "_vortex.txt").c_str(), "w");
+    fprintf(t, "found %d\n", found);
+    fclose(t);
+    return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -82,6 +119,7 @@ int main(int argc, char** argv) {
         size_t eq = a.find('=');
         if (eq != std::string::npos) g_kv[a.substr(0, eq)] = a.substr(eq + 1);
     }
+    if (get("mode", "") == "vortex") return vortex_mode();
     const int dim = geti("dim", 2);
     const int n = geti("n", 64);
     const int gsteps = geti("gsteps", 0), esteps = geti("esteps", 0);

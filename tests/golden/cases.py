@@ -100,3 +100,57 @@ def harness_args(c, psi0_path, out_prefix, data_dir):
          "esteps=%d" % c["esteps"], "energy_every=%d" % c["energy_every"],
          "psi0=" + psi0_path, "out=" + out_prefix, "data=" + data_dir]
     return a
+
+
+# 2D states for the vortex finder (Tracker::findVortex): square n x n grids,
+# x fastest, with GPUE's x grid.  "imprint" multiplies a Gaussian by
+# (x - xk) + i qk (y - yk) factors at seeded positions (charges +-1; one of
+# them sits exactly on a grid node, so psi is 0 there), plus 1% noise;
+# "noise" is a random phase field whose plaquettes wind often and in
+# neighbouring pairs, exercising the rule that skips the plaquette after a
+# mark; "ring" puts the search radius through a ring of vortices.
+VORTEX_CASES = {
+    "vtx_imprint_n128": dict(n=128, box=8.0, radius=5.0, seed=31, kind="imprint", nv=14),
+    "vtx_noise_n64": dict(n=64, box=6.0, radius=4.5, seed=32, kind="noise"),
+    "vtx_ring_n96": dict(n=96, box=8.0, radius=3.0, seed=33, kind="ring", nv=10),
+    "vtx_imprint_n256": dict(n=256, box=10.0, radius=9.0, seed=34, kind="imprint", nv=40),
+}
+
+
+def grid_x(n, box):
+    """generate_p_space's x: -box + i dx on the first half, i dx on the second."""
+    dx = box / (n >> 1)
+    x = np.empty(n)
+    h = n // 2
+    x[:h] = -box + np.arange(h) * dx
+    x[h:] = np.arange(h) * dx
+    return x
+
+
+def vortex_psi(v):
+    """complex128 (n, n) [y, x] state of a VORTEX_CASES entry."""
+    n, box = v["n"], v["box"]
+    rng = np.random.Generator(np.random.PCG64(v["seed"]))
+    x = grid_x(n, box)
+    X, Y = np.meshgrid(x, x)
+    if v["kind"] == "noise":
+        amp = 0.5 + rng.random((n, n))
+        return np.ascontiguousarray(amp * np.exp(2j * np.pi * rng.random((n, n))))
+    psi = np.exp(-(X * X + Y * Y) / (0.5 * box) ** 2).astype(np.complex128)
+    if v["kind"] == "ring":
+        ang = 2 * np.pi * np.arange(v["nv"]) / v["nv"] + 0.1
+        pos = np.stack([v["radius"] * np.cos(ang), v["radius"] * np.sin(ang)], 1)
+        q = np.where(np.arange(v["nv"]) % 2 == 0, 1, -1)
+    else:
+        pos = (rng.random((v["nv"], 2)) - 0.5) * 1.4 * box
+        pos[0] = (x[n // 2 + 3], x[n // 2 - 5])  # on a grid node
+        q = rng.choice([-1, 1], v["nv"])
+    for (xk, yk), qk in zip(pos, q):
+        psi *= (X - xk) + 1j * qk * (Y - yk)
+    psi *= 1.0 + 0.01 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    return np.ascontiguousarray(psi / np.abs(psi).max())
+
+
+def vortex_harness_args(v, psi0_path, out_prefix):
+    return ["mode=vortex", "n=%d" % v["n"], "box=%r" % v["box"], "radius=%r" % v["radius"],
+            "psi0=" + psi0_path, "out=" + out_prefix]

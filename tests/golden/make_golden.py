@@ -7,6 +7,10 @@ set_variables, evolve and energy_calc), and stores the final wavefunction and
 energy as ``<case>.npz`` in --outdir, plus the harness wall time.
 
     python tests/golden/make_golden.py --outdir tests/golden [case ...]
+
+With --vortex it instead runs the harness's host-only findVortex mode (no GPU
+needed) on each VORTEX_CASES state and stores the marker array and the count
+as ``<case>.npz``.
 """
 
 import argparse
@@ -60,6 +64,27 @@ def run_case(name, outdir):
     print(json.dumps(dict(case=name, energy=info["energy"], wall_s=round(wall, 3))))
 
 
+def run_vortex_case(name, outdir):
+    v = cases.VORTEX_CASES[name]
+    psi = cases.vortex_psi(v)
+    with tempfile.TemporaryDirectory() as td:
+        p0 = os.path.join(td, "psi0.bin")
+        psi.tofile(p0)
+        prefix = os.path.join(td, "out")
+        r = subprocess.run([HARNESS] + cases.vortex_harness_args(v, p0, prefix),
+                           stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True,
+                           timeout=600)
+        if r.returncode != 0:
+            print(r.stdout[-3000:])
+            raise RuntimeError("harness failed for %s" % name)
+        marker = np.fromfile(prefix + "_vortex.bin", dtype=np.int32).reshape(psi.shape)
+        found = int(open(prefix + "_vortex.txt").read().split()[1])
+    meta = dict(case=name, params=v, input_sha=cases.checksum(psi), found=found)
+    np.savez_compressed(os.path.join(outdir, name + ".npz"), marker=marker.astype(np.int8),
+                        meta=np.array(json.dumps(meta)))
+    print(json.dumps(dict(case=name, found=found)))
+
+
 def time_case(name, steps):
     """Time GPUE's evolve() on a full-size configuration (no fixture kept)."""
     c = cases.case(name)
@@ -89,8 +114,15 @@ def main():
     ap.add_argument("--outdir", default=HERE)
     ap.add_argument("--timing", action="store_true",
                     help="time GPUE's evolve on the full-size configurations instead")
+    ap.add_argument("--vortex", action="store_true",
+                    help="findVortex fixtures (host code only, no GPU)")
     ap.add_argument("names", nargs="*")
     a = ap.parse_args()
+    if a.vortex:
+        os.makedirs(a.outdir, exist_ok=True)
+        for name in (a.names or list(cases.VORTEX_CASES)):
+            run_vortex_case(name, a.outdir)
+        return
     if a.timing:
         for name, steps in cases.TIMING:
             time_case(name, steps)

@@ -65,6 +65,7 @@ def test_invalid_arguments_fail_without_touching_the_device():
     assert L.gpue_set_operators(None, 0) == 1
     obs = G.Observables()
     assert L.gpue_observables_get(None, ctypes.byref(obs)) == 1
+    assert L.gpue_find_vortices(None, 1.0, None, 0, None, 0, None) == 1
     # batches: argument checks come before any device call
     out = ctypes.c_void_p()
     assert L.gpue_batch_create(None, 1, ctypes.byref(out)) == 1

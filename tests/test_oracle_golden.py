@@ -2,13 +2,16 @@
 
 The fixtures were produced by tests/golden/make_golden.py running the
 reference's parseArgs/init/set_variables/evolve/energy_calc on a B200.  This
-pins the FP64 restatement before it is trusted as the checker.
+pins the FP64 restatement before it is trusted as the checker.  The vortex
+fixtures come from the same build's host-side Tracker::findVortex.
 """
+import os
+
 import numpy as np
 import pytest
 
 import cases
-from helpers import l2, load_golden, oracle_problem, steps_gstate
+from helpers import GOLDEN, l2, load_golden, oracle_problem, steps_gstate
 
 
 @pytest.mark.parametrize("name", cases.FIXTURES)
@@ -62,3 +65,21 @@ def test_oracle_fft_kats():
         assert abs(np.sum(abs(Y) ** 2) / n - np.sum(abs(y) ** 2)) <= 1e-12 * np.sum(abs(y) ** 2)
         assert np.allclose(Y, np.fft.fft(y), atol=1e-12 * n)
         assert np.allclose(oracle.fft1d(Y, +1) / n, y, atol=1e-14)
+
+
+@pytest.mark.parametrize("name", sorted(cases.VORTEX_CASES))
+def test_oracle_find_vortex_matches_reference(name):
+    """The findVortex restatement against markers written by GPUE's own
+    Tracker::findVortex (make_golden.py --vortex)."""
+    import json
+    import oracle
+    d = np.load(os.path.join(GOLDEN, name + ".npz"))
+    meta = json.loads(str(d["meta"]))
+    v = cases.VORTEX_CASES[name]
+    psi = cases.vortex_psi(v)
+    assert cases.checksum(psi) == meta["input_sha"]
+    marker, winding, found = oracle.find_vortex(psi, cases.grid_x(v["n"], v["box"]),
+                                                v["radius"])
+    assert found == meta["found"]
+    assert np.array_equal(marker, d["marker"].astype(np.int32))
+    assert np.array_equal(np.abs(winding), marker)
