@@ -194,6 +194,7 @@ def lib():
         L.gpue_batch_evolve.argtypes = [vp, i32, C.POINTER(BatchOpts), C.POINTER(BatchResult),
                                         C.POINTER(BatchStats)]
         L.gpue_set_gauge_tables.argtypes = [vp, vp, vp, vp]
+        L.gpue_set_potential_table.argtypes = [vp, vp]
         L.gpue_autotune.argtypes = [vp, i32]
         L.gpue_get_plan.argtypes = [vp, i32, C.POINTER(PlanInfo)]
         L.gpue_server_create.argtypes = [C.POINTER(ServerOpts), C.POINTER(vp)]
@@ -215,7 +216,7 @@ def lib():
                      "gpue_load_param_text", "gpue_ast_parse", "gpue_batch_create",
                      "gpue_batch_destroy", "gpue_batch_evolve", "gpue_autotune",
                      "gpue_get_plan", "gpue_set_gauge_tables", "gpue_observables_get",
-                     "gpue_find_vortices"):
+                     "gpue_find_vortices", "gpue_set_potential_table"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -397,6 +398,14 @@ class Solver:
                                  % (a.size, np.prod(self.shape)))
         ptr = [None if a is None else a.ctypes.data for a in keep]
         self._ck(lib().gpue_set_gauge_tables(self._h, *ptr))
+
+    def set_potential_table(self, V):
+        """Full-field potential V (GPUE's V_gpu, e.g. -v torus), x fastest."""
+        v = np.ascontiguousarray(V, dtype=np.float64).ravel()
+        if v.size != int(np.prod(self.shape)):
+            raise ValueError("potential table has %d points, grid has %d"
+                             % (v.size, np.prod(self.shape)))
+        self._ck(lib().gpue_set_potential_table(self._h, v.ctypes.data))
 
     def load_param_text(self, text, time_mode=0, doubles=None):
         """Parameter-file fields (GPUE's -I file) from "name = expr" lines."""

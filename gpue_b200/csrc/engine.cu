@@ -1283,6 +1283,29 @@ gpue_status gpue_set_gauge_tables(gpue_ctx* c, const double* Ax, const double* A
     return GPUE_OK;
 }
 
+gpue_status gpue_set_potential_table(gpue_ctx* c, const double* V) {
+    if (!c || !V) return GPUE_ERR_INVALID_ARG;
+    CK(cudaSetDevice(c->device));
+    if (!c->vtab) {
+        CK(cudaMalloc(&c->vtab, c->N * sizeof(double)));
+        for (auto& t : c->atab) {
+            CK(cudaMalloc(&t, c->N * sizeof(double)));
+            CK(cudaMemset(t, 0, c->N * sizeof(double)));
+        }
+        for (bool& nz : c->atab_nonzero) nz = false;
+        c->use_atab = false;
+    }
+    CK(cudaMemcpy(c->vtab, V, c->N * sizeof(double), cudaMemcpyHostToDevice));
+    // the table replaces a parameter-file V expression
+    c->prog_off[0] = -1;
+    c->prog_len[0] = 0;
+    c->time_dep = false;
+    for (int k = 1; k < 5; ++k) c->time_dep |= c->prog_len[k] > 0;
+    c->ext = true;
+    destroy_graphs(c);
+    return GPUE_OK;
+}
+
 gpue_status gpue_ast_parse(const char* expr, const char* const* names, const double* values,
                            int32_t nvalues, void* nodes_out, int32_t cap, int32_t* count) {
     if (!expr || !count || cap < 0 || nvalues < 0) return GPUE_ERR_INVALID_ARG;

@@ -43,6 +43,85 @@ std::string filecheck(const std::string& f) {
     return f;
 }
 
+// Position of flat index g = i + xDim*(j + yDim*k) (x fastest).
+struct Point {
+    double x, y, z;
+};
+Point point(const Grid& par, size_t g) {
+    const size_t nx = par.ival("xDim"), ny = par.ival("yDim");
+    return {par.x[g % nx], par.y[(g / nx) % ny], par.z[g / (nx * ny)]};
+}
+
+// Full-field Ax, Ay, Az for the gauge of -A (Grid::set_A_fn, src/ds.cu:300-331;
+// generate_gauge, src/operators.cu:471-615): the field kernels of
+// src/operators.cu:621-720 evaluated on the host, or file_A
+// (src/operators.cu:259-270) for -A file.  In 2D, Az is zero and the presets
+// see zMax = 1 (generate_gauge's default).
+void gauge_tables(const Grid& par, std::vector<double> (&A)[3]) {
+    const int dimnum = par.ival("dimnum");
+    const size_t n = (size_t)par.ival("xDim") * par.ival("yDim") * par.ival("zDim");
+    for (auto& a : A) a.assign(n, 0.0);
+    const double omega = par.dval("omega"), omegaX = par.dval("omegaX"),
+                 omegaY = par.dval("omegaY");
+    const double xMax = par.dval("xMax"), yMax = par.dval("yMax");
+    const double zMax = dimnum == 3 ? par.dval("zMax") : 1.0;
+    if (par.Afn == "file") {
+        const char* keys[3] = {"Axfile", "Ayfile", "Azfile"};
+        for (int a = 0; a < (dimnum == 3 ? 3 : 2); ++a) {
+            std::ifstream in(par.sval(keys[a]));
+            std::vector<double> v;
+            double t;
+            while (in >> t) v.push_back(omega * t);
+            if (v.size() != n)
+                throw std::runtime_error(par.sval(keys[a]) + " has " + std::to_string(v.size()) +
+                                         " values, the grid " + std::to_string(n));
+            A[a] = v;
+        }
+        return;
+    }
+    for (size_t g = 0; g < n; ++g) {
+        const Point q = point(par, g);
+        if (par.Afn == "rotation") {  // krotation_Ax / krotation_Ay
+            A[0][g] = -q.y * omega * omegaX;
+            A[1][g] = q.x * omega * omegaY;
+        } else if (par.Afn == "ring_rotation") {  // kring_rotation_A{x,y,z}
+            const double theta = std::atan2(q.y, q.x);
+            A[0][g] = (q.z + zMax) * std::cos(theta) * omega * omegaX;
+            A[1][g] = (q.z + zMax) * std::sin(theta) * omega * omegaX;
+            if (dimnum == 3) A[2][g] = std::sqrt(q.x * q.x + q.y * q.y) * omega * omegaX;
+        } else if (par.Afn == "ring") {  // kring_Az
+            const double rad = std::sqrt(q.x * q.x + q.y * q.y);
+            if (dimnum == 3) A[2][g] = omega * std::exp(-rad * rad / (0.0001 * xMax)) * 0.01;
+        } else if (par.Afn == "test") {  // ktest_Ax
+            A[0][g] = (std::sin(q.y * 100000) + 1) * yMax * omega;
+        }
+    }
+}
+
+// ktorus_V (src/operators.cu:1011-1029) with GPUE's items array
+// (src/operators.cu:753-792): omegaZ and z0_shift only in 3D.
+std::vector<double> torus_V(const Grid& par, const std::vector<double> (&A)[3]) {
+    const int dimnum = par.ival("dimnum");
+    const size_t n = A[0].size();
+    const double xMax = par.dval("xMax"), omegaX = par.dval("omegaX"),
+                 omegaY = par.dval("omegaY"), mass = par.dval("mass"),
+                 fudge = par.dval("fudge");
+    const double omegaZ = dimnum == 3 ? par.dval("omegaZ") : 0.0;
+    const double x0 = par.dval("x0_shift"), y0 = par.dval("y0_shift");
+    const double z0 = dimnum == 3 ? par.dval("z0_shift") : 0.0;
+    std::vector<double> V(n);
+    for (size_t g = 0; g < n; ++g) {
+        const Point q = point(par, g);
+        const double rad = std::sqrt((q.x - x0) * (q.x - x0) + (q.y - y0) * (q.y - y0)) -
+                           0.5 * xMax;
+        const double omegaR = omegaX * omegaX + omegaY * omegaY;
+        const double V_tot = 2 * omegaZ * omegaZ * (q.z - z0) * (q.z - z0) +
+                             omegaR * (rad * rad + fudge * rad * q.z);
+        V[g] = 0.5 * mass * (V_tot + A[0][g] * A[0][g] + A[1][g] * A[1][g] + A[2][g] * A[2][g]);
+    }
+    return V;
+}
+
 // The context of this Grid, created on first use from its keys; a
 // parameter file (-I) is loaded into it with the Grid's doubles as names.
 gpue_ctx* ensure_ctx(Grid& par) {
@@ -71,23 +150,22 @@ gpue_ctx* ensure_ctx(Grid& par) {
                                    (int32_t)names.size()),
               c, "parameter file");
     }
-    if (par.Afn == "file") {
-        // file_A (src/operators.cu:259-270): whitespace-separated values times omega
-        const size_t n = (size_t)par.ival("xDim") * par.ival("yDim") * par.ival("zDim");
+    const bool table_a = par.Afn == "file" || par.Afn == "ring_rotation" ||
+                         par.Afn == "ring" || par.Afn == "test";
+    if (table_a || par.Vfn == "torus") {
+        if (par.bval("use_param_file"))
+            throw std::runtime_error("-A " + par.Afn + " / -v " + par.Vfn +
+                                     " tables are not combined with a parameter file");
         std::vector<double> A[3];
-        const char* keys[3] = {"Axfile", "Ayfile", "Azfile"};
-        for (int a = 0; a < (par.ival("dimnum") == 3 ? 3 : 2); ++a) {
-            std::ifstream in(par.sval(keys[a]));
-            double v;
-            while (in >> v) A[a].push_back(par.dval("omega") * v);
-            if (A[a].size() != n)
-                throw std::runtime_error(par.sval(keys[a]) + " has " +
-                                         std::to_string(A[a].size()) + " values, the grid " +
-                                         std::to_string(n));
+        gauge_tables(par, A);
+        if (table_a)
+            check(gpue_set_gauge_tables(c, A[0].data(), A[1].data(),
+                                        par.ival("dimnum") == 3 ? A[2].data() : nullptr),
+                  c, "gauge tables");
+        if (par.Vfn == "torus") {
+            const std::vector<double> V = torus_V(par, A);
+            check(gpue_set_potential_table(c, V.data()), c, "torus potential");
         }
-        check(gpue_set_gauge_tables(c, A[0].data(), A[1].data(),
-                                    A[2].empty() ? nullptr : A[2].data()),
-              c, "gauge from file");
     }
     if (par.bval("autotune")) check(gpue_autotune(c, 0), c, "gpue_autotune");
     return c;
@@ -292,13 +370,14 @@ void init(Grid& par) {
     const int dimnum = par.ival("dimnum");
     if (dimnum != 2 && dimnum != 3)
         throw std::runtime_error("this build runs 2D and 3D grids (-c 2 or -c 3)");
-    if (par.Afn != "rotation" && par.Afn != "constant" && par.Afn != "file")
+    static const char* gauges[] = {"rotation", "constant", "file", "ring_rotation", "ring",
+                                   "test"};
+    if (std::find(std::begin(gauges), std::end(gauges), par.Afn) == std::end(gauges))
         throw std::runtime_error("gauge field '" + par.Afn +
-                                 "' is not built; use rotation, constant, file or a "
-                                 "parameter file");
-    if (par.Vfn != "2d" && par.Vfn != "3d")
-        throw std::runtime_error("potential '" + par.Vfn +
-                                 "' is not built; use the harmonic trap or a parameter file");
+                                 "' is not one of rotation, constant, file, ring_rotation, "
+                                 "ring, test");
+    if (par.Vfn != "2d" && par.Vfn != "3d" && par.Vfn != "torus")
+        throw std::runtime_error("potential '" + par.Vfn + "' is not one of 2d, 3d, torus");
     const int N = par.ival("atoms");
     const int xDim = par.ival("xDim"), yDim = par.ival("yDim"), zDim = par.ival("zDim");
     const double omegaX = par.dval("omegaX"), omegaY = par.dval("omegaY"),
@@ -369,6 +448,18 @@ void init(Grid& par) {
             for (int j = 0; j < yDim; ++j)
                 for (int i = 0; i < xDim; ++i) {
                     const size_t g = i + (size_t)xDim * (j + (size_t)yDim * k);
+                    if (par.Wfcfn == "torus") {
+                        // ktorus_wfc (src/operators.cu:1052-1067)
+                        const double x0 = par.dval("x0_shift"), y0 = par.dval("y0_shift");
+                        const double rad = std::sqrt((par.x[i] - x0) * (par.x[i] - x0) +
+                                                     (par.y[j] - y0) * (par.y[j] - y0)) -
+                                           0.5 * xMax;
+                        const double az = dimnum == 3 ? a0z : 1.0;
+                        par.wfc[g] = std::exp(-(std::pow(rad / (Rxy * a0x * 0.5), 2) +
+                                                std::pow(par.z[k] / (Rxy * az * 0.5), 2)));
+                        sum += std::abs(par.wfc[g]);
+                        continue;
+                    }
                     const double phi = -std::fmod(winding * std::atan2(par.y[j], par.x[i]), 2 * kPI);
                     const double e = std::exp(-(par.x[i] * par.x[i] / (Rxy * Rxy * a0x * a0x) +
                                                 par.y[j] * par.y[j] / (Rxy * Rxy * a0y * a0y) +
@@ -432,6 +523,29 @@ double energy_calc(Grid& par) {
 
 // --------------------------------------------------------------- evolve --
 
+// Tracker::findVortex on the resident state with radius mask_2d; prints the
+// count as evolve() does and, when writing, the marks as vort_mark_<step>:
+// one line "row,column,marker,winding" per marked plaquette (row = y index,
+// column = x index, the marker index row*xDim + column), in findVortex's
+// visiting order.
+static void find_vortices(Grid& par, gpue_ctx* c, int step, bool write_it) {
+    const double radius = par.dval("mask_2d");
+    int32_t found = 0;
+    check(gpue_find_vortices(c, radius, nullptr, GPUE_MEM_HOST, nullptr, 0, &found), c,
+          "findVortex");
+    std::printf("Located %d vortices\n", found);
+    if (!write_it) return;
+    std::vector<gpue_vortex> v((size_t)found);
+    if (found > 0)
+        check(gpue_find_vortices(c, radius, nullptr, GPUE_MEM_HOST, v.data(), found, &found),
+              c, "findVortex");
+    std::ofstream out(par.sval("data_dir") + "vort_mark_" + std::to_string(step));
+    out << "#ROW,COLUMN,MARKER,WINDING\n";
+    for (const gpue_vortex& m : v)
+        out << m.i << ',' << m.j << ',' << m.marker << ',' << m.winding << '\n';
+}
+
+
 int evolve(Grid& par, int numSteps, unsigned gstate, const std::string& /*buffer*/) {
     gpue_ctx* c = ensure_ctx(par);
     check(gpue_set_wfc(c, par.wfc.data(), GPUE_MEM_HOST, GPUE_C128), c, "gpue_set_wfc");
@@ -452,6 +566,10 @@ int evolve(Grid& par, int numSteps, unsigned gstate, const std::string& /*buffer
     o.energy_calc_steps = every;
     o.energy_calc_threshold = par.dval("energy_calc_threshold");
     o.norm_guard = -1;
+    // 2D real time: findVortex at every print step (src/evolution.cu:483-486),
+    // on the device; the later lattice analysis (vortPos/lsFit and the
+    // optical lattice, src/evolution.cu:487-703) is not part of this build
+    const bool track = gstate == 1 && par.ival("dimnum") == 2 && p > 0;
     int i = 0;
     bool stopped = false;
     while (i < numSteps && !stopped) {
@@ -459,9 +577,10 @@ int evolve(Grid& par, int numSteps, unsigned gstate, const std::string& /*buffer
             check(gpue_get_wfc(c, par.wfc.data(), GPUE_MEM_HOST, GPUE_C128), c, "gpue_get_wfc");
             fileio::write_out(fname, par.wfc, i);
         }
-        // one call up to the next write point or just past the next check
+        if (track && i % p == 0) find_vortices(par, c, i, write_it);
+        // one call up to the next print point or just past the next check
         int next = numSteps;
-        if (write_it && p > 0) next = std::min(next, (i / p + 1) * p);
+        if ((write_it || track) && p > 0) next = std::min(next, (i / p + 1) * p);
         int check_step = -1;
         if (every > 0) {
             const int nc = ((i + every - 1) / every) * every;

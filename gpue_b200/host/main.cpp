@@ -33,6 +33,9 @@ int main(int argc, char** argv) {
             std::printf("ramp=%d\nramp_type=%d\nprecision=%d\n", p.ramp, p.ramp_type,
                         p.precision);
             std::printf("gsteps=%d\nesteps=%d\n", par.ival("gsteps"), par.ival("esteps"));
+            for (const char* k : {"x0_shift", "y0_shift", "z0_shift", "fudge", "Rxy", "a0x",
+                                  "a0y", "a0z", "dx", "dy", "dz"})
+                std::printf("%s=%.17g\n", k, par.dval(k));
             std::printf("energy_calc_steps=%d\nenergy_calc_threshold=%.17g\n",
                         par.bval("energy_calc") ? par.ival("energy_calc_steps") : -1,
                         par.dval("energy_calc_threshold"));

@@ -243,6 +243,14 @@ gpue_status gpue_ast_parse(const char* expr, const char* const* names, const dou
 gpue_status gpue_set_gauge_tables(gpue_ctx* ctx, const double* Ax, const double* Ay,
                                   const double* Az);
 
+/* A full-field potential V (host array of xDim*yDim*zDim doubles, x fastest)
+ * in place of the harmonic trap: GPUE's V_gpu as generate_fields leaves it
+ * (src/operators.cu:800-831), e.g. ktorus_V for -v torus (src/operators.cu:
+ * 1011-1029), including any m|A|^2/2 term.  Call it after
+ * gpue_set_gauge_tables, which recomputes the harmonic V.  It also replaces
+ * a parameter-file V expression. */
+gpue_status gpue_set_potential_table(gpue_ctx* ctx, const double* V);
+
 /* Device pointer of the resident wavefunction and its dtype (GPUE_C128/C64). */
 gpue_status gpue_ctx_wfc_device(gpue_ctx* ctx, void** psi, int32_t* dtype);
 

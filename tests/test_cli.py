@@ -100,8 +100,9 @@ def test_read_wfc_files(tmp_path):
 @pytest.mark.parametrize("args,msg", [
     (["-r"], "wfc_load"),                       # -r without the input files
     (["-A", "file"], "Axgauge"),                # -A file without the gauge files
-    (["-A", "ring"], "gauge field"),
-    (["-v", "torus"], "potential"),
+    (["-A", "spiral"], "gauge field"),
+    (["-v", "box"], "potential"),
+    (["-A", "ring", "-I", "params.cfg"], "params.cfg"),
     (["-c", 1], "2D and 3D"),
     (["--no-such-option"], "unknown option"),
 ])

@@ -67,3 +67,40 @@ def test_cli_early_stop_and_autotune(tmp_path):
     # GPUE writes energyi.dat with 6 significant digits (the stream default),
     # so the last two printed values agree to that precision
     assert abs(E[-1] - E[-2]) <= 1.5e-5 * abs(E[-2])
+
+
+def test_cli_finds_vortices_at_print_steps(tmp_path):
+    """2D real time: findVortex runs on the device at every print step; the
+    marks written (vort_mark_<step>) equal the oracle's findVortex on the
+    wfc_ev_<step> state written at the same step."""
+    import cases
+    import oracle
+    from cli_helpers import write_wfc
+    n, radius_frac = 128, 0.7
+    base = ["-x", n, "-y", n, "-s", "-i", 100, "-l", "-w", 0.4, "-g", 0, "-e", 25, "-W",
+            "-p", 10, "-r"]
+    probe = tmp_path / "probe"
+    probe.mkdir()
+    xmax = params(["-x", n, "-y", n], probe)["xMax"]
+    x = cases.grid_x(n, xmax)
+    X, Y = np.meshgrid(x, x)
+    psi = np.exp(-(X ** 2 + Y ** 2) / (0.4 * xmax) ** 2).astype(np.complex128)
+    rng = np.random.Generator(np.random.PCG64(77))
+    for (xk, yk), q in zip((rng.random((6, 2)) - 0.5) * 0.8 * xmax, (1, -1, 1, 1, -1, 1)):
+        psi *= (X - xk) + 1j * q * (Y - yk)
+    psi /= np.sqrt(np.sum(np.abs(psi) ** 2) * (x[1] - x[0]) ** 2)
+    write_wfc(tmp_path, psi)
+    radius = radius_frac * xmax
+    out = run(base + ["-m", radius], tmp_path).stdout
+    located = [int(l.split()[1]) for l in out.splitlines() if l.startswith("Located")]
+    assert len(located) == 3  # steps 0, 10, 20
+    for k, step in enumerate((0, 10, 20)):
+        state = read_wfc(tmp_path, "wfc_ev", step, (n, n))
+        marker, winding, found = oracle.find_vortex(state, x, radius)
+        rows = np.loadtxt(tmp_path / ("vort_mark_%d" % step), delimiter=",", comments="#",
+                          dtype=np.int64, ndmin=2)
+        assert found == located[k] == len(rows) > 0
+        ii, jj = np.nonzero(marker)
+        assert np.array_equal(rows[:, 0], ii) and np.array_equal(rows[:, 1], jj)
+        assert np.array_equal(rows[:, 2], marker[ii, jj])
+        assert np.array_equal(rows[:, 3], winding[ii, jj])
