@@ -195,6 +195,8 @@ def lib():
                                         C.POINTER(BatchStats)]
         L.gpue_set_gauge_tables.argtypes = [vp, vp, vp, vp]
         L.gpue_set_potential_table.argtypes = [vp, vp]
+        L.gpue_snapshot_save.argtypes = [vp, C.c_char_p, i32, C.c_int64]
+        L.gpue_snapshot_load.argtypes = [vp, C.c_char_p, C.POINTER(i32), C.POINTER(C.c_int64)]
         L.gpue_autotune.argtypes = [vp, i32]
         L.gpue_get_plan.argtypes = [vp, i32, C.POINTER(PlanInfo)]
         L.gpue_server_create.argtypes = [C.POINTER(ServerOpts), C.POINTER(vp)]
@@ -216,7 +218,8 @@ def lib():
                      "gpue_load_param_text", "gpue_ast_parse", "gpue_batch_create",
                      "gpue_batch_destroy", "gpue_batch_evolve", "gpue_autotune",
                      "gpue_get_plan", "gpue_set_gauge_tables", "gpue_observables_get",
-                     "gpue_find_vortices", "gpue_set_potential_table"):
+                     "gpue_find_vortices", "gpue_set_potential_table", "gpue_snapshot_save",
+                     "gpue_snapshot_load"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -398,6 +401,16 @@ class Solver:
                                  % (a.size, np.prod(self.shape)))
         ptr = [None if a is None else a.ctypes.data for a in keep]
         self._ck(lib().gpue_set_gauge_tables(self._h, *ptr))
+
+    def save_snapshot(self, path, gstate=0, step=0):
+        """Binary snapshot of the state for checkpoint/resume (gpue_snapshot_save)."""
+        self._ck(lib().gpue_snapshot_save(self._h, os.fsencode(path), int(gstate), int(step)))
+
+    def load_snapshot(self, path):
+        """Load a snapshot (gpue_snapshot_load); returns (gstate, step)."""
+        g, st = C.c_int32(), C.c_int64()
+        self._ck(lib().gpue_snapshot_load(self._h, os.fsencode(path), C.byref(g), C.byref(st)))
+        return g.value, st.value
 
     def set_potential_table(self, V):
         """Full-field potential V (GPUE's V_gpu, e.g. -v torus), x fastest."""

@@ -239,6 +239,9 @@ Grid parse_args(int argc, char** argv) {
     par.store("precision", (int)GPUE_PREC_FP64);
     par.store("autotune", false);
     par.store("print_params", false);
+    par.store("checkpoint_every", 0);
+    par.store("resume", false);
+    par.store("start_step", 0);
 
     // long options first; the rest go to getopt as GPUE parses them
     std::vector<char*> args;
@@ -249,6 +252,9 @@ Grid parse_args(int argc, char** argv) {
         else if (a == "--precision=fp64") par.store("precision", (int)GPUE_PREC_FP64);
         else if (a == "--autotune") par.store("autotune", true);
         else if (a == "--print-params") par.store("print_params", true);
+        else if (a.rfind("--checkpoint-every=", 0) == 0)
+            par.store("checkpoint_every", std::atoi(a.c_str() + 19));
+        else if (a == "--resume") par.store("resume", true);
         else if (a.rfind("--", 0) == 0) throw std::runtime_error("unknown option " + a);
         else args.push_back(argv[i]);
     }
@@ -546,9 +552,24 @@ static void find_vortices(Grid& par, gpue_ctx* c, int step, bool write_it) {
 }
 
 
+std::pair<int, int> resume_snapshot(Grid& par) {
+    gpue_ctx* c = ensure_ctx(par);
+    const std::string path = filecheck(par.sval("data_dir") + "snapshot.bin");
+    int32_t g = 0;
+    int64_t step = 0;
+    check(gpue_snapshot_load(c, path.c_str(), &g, &step), c, "resume");
+    std::printf("Resuming %s-time evolution at step %lld\n", g == 0 ? "imaginary" : "real",
+                (long long)step);
+    return {g, (int)step};
+}
+
 int evolve(Grid& par, int numSteps, unsigned gstate, const std::string& /*buffer*/) {
     gpue_ctx* c = ensure_ctx(par);
-    check(gpue_set_wfc(c, par.wfc.data(), GPUE_MEM_HOST, GPUE_C128), c, "gpue_set_wfc");
+    const int start = par.ival("start_step");
+    par.store("start_step", 0);  // applies to this call only
+    if (start == 0)
+        check(gpue_set_wfc(c, par.wfc.data(), GPUE_MEM_HOST, GPUE_C128), c, "gpue_set_wfc");
+    const int ckpt = par.ival("checkpoint_every");
     const std::string data_dir = par.sval("data_dir");
     const int p = par.ival("printSteps");
     const bool write_it = par.bval("write_it");
@@ -570,9 +591,12 @@ int evolve(Grid& par, int numSteps, unsigned gstate, const std::string& /*buffer
     // on the device; the later lattice analysis (vortPos/lsFit and the
     // optical lattice, src/evolution.cu:487-703) is not part of this build
     const bool track = gstate == 1 && par.ival("dimnum") == 2 && p > 0;
-    int i = 0;
+    int i = start;
     bool stopped = false;
     while (i < numSteps && !stopped) {
+        if (ckpt > 0 && i > start && i % ckpt == 0)
+            check(gpue_snapshot_save(c, (data_dir + "snapshot.bin").c_str(), (int32_t)gstate, i),
+                  c, "snapshot");
         if (write_it && p > 0 && i % p == 0) {  // the state after i steps
             check(gpue_get_wfc(c, par.wfc.data(), GPUE_MEM_HOST, GPUE_C128), c, "gpue_get_wfc");
             fileio::write_out(fname, par.wfc, i);
@@ -581,6 +605,7 @@ int evolve(Grid& par, int numSteps, unsigned gstate, const std::string& /*buffer
         // one call up to the next print point or just past the next check
         int next = numSteps;
         if ((write_it || track) && p > 0) next = std::min(next, (i / p + 1) * p);
+        if (ckpt > 0) next = std::min(next, (i / ckpt + 1) * ckpt);
         int check_step = -1;
         if (every > 0) {
             const int nc = ((i + every - 1) / every) * every;

@@ -6,6 +6,7 @@
 #pragma once
 
 #include <string>
+#include <utility>
 
 #include "grid.h"
 
@@ -36,7 +37,15 @@ void set_variables(Grid& par, int ev_type);
 // as GPUE names it (wfc_0_const_<i>, wfc_ev_<i>, ...); with energy_calc, the
 // check energies are appended to energyi.dat / energy.dat and "energy" holds
 // the last one.  Returns the steps run.
+// With checkpoint_every = K > 0 a binary snapshot (gpue_snapshot_save) of
+// the state after every K-th step goes to <data_dir>snapshot.bin; with
+// "start_step" = s > 0 the loop starts at step s on the state the context
+// already holds (a resumed run) instead of reading par.wfc.
 int evolve(Grid& par, int numSteps, unsigned gstate, const std::string& buffer);
+
+// --resume: loads <data_dir>snapshot.bin into the context; returns its phase
+// (0 imaginary, 1 real) and step.
+std::pair<int, int> resume_snapshot(Grid& par);
 
 // energy_calc(par, wfc) (src/split_op.cu:208-375) of the current state.
 double energy_calc(Grid& par);

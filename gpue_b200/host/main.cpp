@@ -1,8 +1,11 @@
 // main.cpp -- the gpue command line: GPUE's main() (src/init.cu:500-568)
-// over the B200 step.  Same flags and files as GPUE; three extra options:
+// over the B200 step.  Same flags and files as GPUE; five extra options:
 //   --precision=fp32   the fused complex64 form (default fp64, the replica)
 //   --autotune         time the FFT plans for this grid before stepping
 //   --print-params     print the parameters the step would use and exit
+//   --checkpoint-every=K  binary snapshot of the state every K steps
+//                      (<data_dir>snapshot.bin, replaced each time)
+//   --resume           continue from <data_dir>snapshot.bin
 #include <chrono>
 #include <cstdio>
 #include <iostream>
@@ -51,7 +54,14 @@ int main(int argc, char** argv) {
             fileio::write_out_double(data_dir + "y", par.y, 0);
             fileio::write_out_double(data_dir + "z", par.z, 0);
         }
-        if (par.ival("gsteps") > 0) {
+        // --resume: continue from <data_dir>snapshot.bin (its phase and step)
+        int phase = 0;
+        if (par.bval("resume")) {
+            const auto r = resume_snapshot(par);
+            phase = r.first;
+            par.store("start_step", r.second);
+        }
+        if (phase == 0 && par.ival("gsteps") > 0) {
             std::cout << "Imaginary-time evolution started..." << '\n';
             set_variables(par, 0);
             evolve(par, par.ival("gsteps"), 0, buffer);

@@ -20,6 +20,8 @@
  *                        wavefunctions by julia/calc_energy.jl:32-66 and
  *                        py/en.py:44-66
  *   gpue_find_vortices   Tracker::findVortex  src/tracker.cu:102-166
+ *   gpue_snapshot_*      binary counterpart of FileIO::writeOut/readIn
+ *                        (src/fileIO.cu:13-72) for checkpoint and resume
  *   gpue_last_error      cudaHandleError/cudaCheckError/cufftHandleError
  *                        (src/split_op.cu:40-59) report-and-exit replaced by
  *                        status codes plus a message
@@ -181,6 +183,23 @@ typedef struct gpue_observables {
 } gpue_observables;
 
 gpue_status gpue_observables_get(gpue_ctx* ctx, gpue_observables* out);
+
+/* Binary snapshots for checkpoint and resume (GPUE only has the text dumps of
+ * FileIO::writeOut/readIn, src/fileIO.cu:13-72, restarted with -r).  A
+ * snapshot holds the state exactly as the context keeps it (the precision it
+ * steps in, the imaginary-time renormalisation still pending, the energy of
+ * the latest check that the next early-stop test compares with), the
+ * gpue_params it belongs to, the caller's phase and step, and a checksum.
+ * Loading it into a context with the same parameters (precision and device
+ * may differ) and continuing with gpue_evolve's step_offset = step repeats
+ * the uninterrupted run bit for bit in the same precision.  Field tables and
+ * parameter-file fields are not part of a snapshot: install them again.
+ * Saves write "<path>.tmp" and rename it over path.  Load fails with
+ * GPUE_ERR_INVALID_ARG for another grid or parameters, a bad header, a short
+ * file or a checksum mismatch. */
+gpue_status gpue_snapshot_save(gpue_ctx* ctx, const char* path, int32_t gstate, int64_t step);
+gpue_status gpue_snapshot_load(gpue_ctx* ctx, const char* path, int32_t* gstate,
+                               int64_t* step);
 
 /* 2D vortex finder: Tracker::findVortex (src/tracker.cu:102-166), which GPUE
  * runs on a host copy of the state at print steps in real time

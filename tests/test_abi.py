@@ -66,6 +66,8 @@ def test_invalid_arguments_fail_without_touching_the_device():
     obs = G.Observables()
     assert L.gpue_observables_get(None, ctypes.byref(obs)) == 1
     assert L.gpue_find_vortices(None, 1.0, None, 0, None, 0, None) == 1
+    assert L.gpue_snapshot_save(None, b"x", 0, 0) == 1
+    assert L.gpue_snapshot_load(None, b"x", None, None) == 1
     # batches: argument checks come before any device call
     out = ctypes.c_void_p()
     assert L.gpue_batch_create(None, 1, ctypes.byref(out)) == 1
