@@ -199,6 +199,8 @@ def lib():
         L.gpue_snapshot_load.argtypes = [vp, C.c_char_p, C.POINTER(i32), C.POINTER(C.c_int64)]
         L.gpue_autotune.argtypes = [vp, i32]
         L.gpue_get_plan.argtypes = [vp, i32, C.POINTER(PlanInfo)]
+        L.gpue_list_plans.argtypes = [i32, i32, C.POINTER(PlanInfo), i32, C.POINTER(i32)]
+        L.gpue_set_plan.argtypes = [vp, i32, i32, i32, i32, i32, i32]
         L.gpue_server_create.argtypes = [C.POINTER(ServerOpts), C.POINTER(vp)]
         L.gpue_server_destroy.argtypes = [vp]
         L.gpue_server_last_error.argtypes = [vp]
@@ -219,7 +221,7 @@ def lib():
                      "gpue_batch_destroy", "gpue_batch_evolve", "gpue_autotune",
                      "gpue_get_plan", "gpue_set_gauge_tables", "gpue_observables_get",
                      "gpue_find_vortices", "gpue_set_potential_table", "gpue_snapshot_save",
-                     "gpue_snapshot_load"):
+                     "gpue_snapshot_load", "gpue_list_plans", "gpue_set_plan"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -227,6 +229,16 @@ def lib():
 
 def supported_length(n, precision=PREC_FP64):
     return bool(lib().gpue_supported_length(precision, n))
+
+
+def list_plans(n, precision=PREC_FP64):
+    """The compiled FFT plans of length n (gpue_list_plans), default first."""
+    cnt = C.c_int32()
+    _check(lib().gpue_list_plans(precision, n, None, 0, C.byref(cnt)))
+    out = (PlanInfo * max(cnt.value, 1))()
+    _check(lib().gpue_list_plans(precision, n, out, cnt.value, C.byref(cnt)))
+    return [{k: out[i].as_dict()[k] for k in ("n", "ra", "rb", "rc", "threads_per_line")}
+            for i in range(cnt.value)]
 
 
 def default_params():
@@ -385,6 +397,11 @@ class Solver:
         """Time the compiled plans and lines-per-CTA choices; keep the fastest."""
         self._ck(lib().gpue_autotune(self._h, 1 if force else 0))
         return [self.plan(a) for a in range(len(self.shape))]
+
+    def set_plan(self, axis, ra, rb, rc, threads_per_line, lines_per_cta=0):
+        """Use one compiled plan on one axis (gpue_set_plan)."""
+        self._ck(lib().gpue_set_plan(self._h, axis, ra, rb, rc, threads_per_line,
+                                     lines_per_cta))
 
     def plan(self, axis):
         out = PlanInfo()

@@ -1357,6 +1357,47 @@ gpue_status gpue_get_plan(gpue_ctx* c, int32_t axis, gpue_plan_info* out) {
     return GPUE_OK;
 }
 
+gpue_status gpue_list_plans(int32_t precision, int32_t n, gpue_plan_info* out, int32_t cap,
+                            int32_t* count) {
+    if (!count || cap < 0 || (cap > 0 && !out) ||
+        (precision != GPUE_PREC_FP32 && precision != GPUE_PREC_FP64))
+        return GPUE_ERR_INVALID_ARG;
+    const PassKernel* ks[8];
+    const int nk = find_pass_kernels(kprec(precision), n, ks, 8);
+    *count = nk;
+    for (int i = 0; i < nk && i < cap; ++i) {
+        std::memset(&out[i], 0, sizeof out[i]);
+        out[i].n = ks[i]->n;
+        out[i].ra = ks[i]->ra;
+        out[i].rb = ks[i]->rb;
+        out[i].rc = ks[i]->rc;
+        out[i].threads_per_line = ks[i]->p;
+    }
+    return GPUE_OK;
+}
+
+gpue_status gpue_set_plan(gpue_ctx* c, int32_t axis, int32_t ra, int32_t rb, int32_t rc,
+                          int32_t p, int32_t lines) {
+    if (!c || axis < 0 || axis >= c->dim || lines < 0) return GPUE_ERR_INVALID_ARG;
+    CK(cudaSetDevice(c->device));
+    const int prec = c->prec;
+    const PassKernel* ks[8];
+    const int nk = find_pass_kernels(kprec(prec), c->ax[axis].n, ks, 8);
+    for (int i = 0; i < nk; ++i) {
+        const PassKernel* k = ks[i];
+        if (k->ra != ra || k->rb != rb || k->rc != rc || k->p != p) continue;
+        LaunchCfg lc;
+        if (!build_cfg(c, prec, axis, k, lines ? lines : default_lines(c, axis, k), lc))
+            return fail(c, GPUE_ERR_INVALID_ARG, "plan (%d,%d,%d) P=%d: %d lines per CTA do not fit",
+                        ra, rb, rc, p, lines);
+        c->lc[prec][axis] = lc;
+        destroy_graphs(c);
+        return GPUE_OK;
+    }
+    return fail(c, GPUE_ERR_INVALID_ARG, "no compiled plan (%d,%d,%d) P=%d for length %d", ra,
+                rb, rc, p, c->ax[axis].n);
+}
+
 gpue_status gpue_evolve(gpue_ctx* c, int32_t nsteps, int32_t gstate,
                         const gpue_evolve_opts* opts, gpue_evolve_result* res) {
     if (!c || nsteps < 0 || (gstate != 0 && gstate != 1)) return GPUE_ERR_INVALID_ARG;

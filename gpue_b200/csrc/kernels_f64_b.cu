@@ -1,8 +1,10 @@
 // kernels_f64_b.cu -- complex128 pass kernels (the plain FP64 form), lengths >= 256.
 //
-// Plans per line length: radix sequence (RA, RA) or (RA, RB, RA) and P
-// threads per line, for E = N/P <= 16 complex values per thread where the
-// length allows it (more resident warps, shorter straight-line code).  The
+// Plans per line length: radix sequence (RA, RA), (RA, RB, RA) or
+// (RA, RB, RC, RA) and P threads per line.  E = N/P values per thread must be
+// a multiple of every radix; the defaults keep E <= 16 where the length
+// allows it and E = 12 or 20 for the radix-3 and radix-5 lengths (more
+// resident warps, shorter straight-line code, fewer spills).  The
 // first plan of a length is the default; the others (fewer threads per line,
 // so a strided pass can take more lines per CTA and read whole 128-byte rows)
 // are candidates for the autotuner.
@@ -14,10 +16,14 @@ static const PassKernel kTable[] = {
     GPUE_PLAN(double, 256, 8, 4, 32),
     GPUE_PLAN(double, 256, 16, 0, 16),
     GPUE_PLAN(double, 320, 4, 20, 16),
+    GPUE_PLAN4(double, 320, 4, 5, 4, 16, 128, 2),
+    GPUE_PLAN4(double, 384, 4, 6, 4, 32, kMaxPassThreads, 2),
     GPUE_PLAN(double, 384, 4, 24, 16),
     GPUE_PLAN(double, 512, 8, 8, 64),
     GPUE_PLAN(double, 512, 8, 8, 32),
+    GPUE_PLAN4(double, 640, 4, 10, 4, 32, 128, 2),
     GPUE_PLAN(double, 640, 8, 10, 16),
+    GPUE_PLAN4(double, 768, 4, 12, 4, 64, kMaxPassThreads, 2),
     GPUE_PLAN(double, 768, 8, 12, 32),
     GPUE_PLAN(double, 1024, 16, 4, 64),
 };

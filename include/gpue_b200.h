@@ -297,6 +297,19 @@ typedef struct gpue_plan_info {
 /* The launch shape the context uses along an axis (0 = x). */
 gpue_status gpue_get_plan(gpue_ctx* ctx, int32_t axis, gpue_plan_info* out);
 
+/* The compiled plans of one line length (n, ra, rb, rc, threads_per_line set;
+ * the first is the default).  *count receives how many exist; at most cap are
+ * written. */
+gpue_status gpue_list_plans(int32_t precision, int32_t n, gpue_plan_info* out, int32_t cap,
+                            int32_t* count);
+
+/* Use the compiled plan (ra, rb, rc, threads_per_line) on one axis of the
+ * context, with lines_per_cta lines per CTA (0: the default count).  Fails
+ * with GPUE_ERR_INVALID_ARG when no such plan exists or the launch shape does
+ * not fit the grid.  Results differ from another plan's only by round-off. */
+gpue_status gpue_set_plan(gpue_ctx* ctx, int32_t axis, int32_t ra, int32_t rb, int32_t rc,
+                          int32_t threads_per_line, int32_t lines_per_cta);
+
 /* No counterpart in GPUE: sum |psi|^2 * dV of a wavefunction the caller owns
  * on the current device, written to *out (device memory the caller owns),
  * for callers that must not trigger any device allocation, such as a server
