@@ -58,7 +58,7 @@ def parse_args():
     ap.add_argument("--quick", action="store_true", help="skip the steady-state and e2e legs")
     ap.add_argument("--only", choices=["batch", "serve", "large"], default=None,
                     help="run one auxiliary leg alone and print its JSON")
-    ap.add_argument("--profile", choices=["fp32", "fp64"], default=None,
+    ap.add_argument("--profile", choices=["fp32", "fp64", "fp32_3d", "fp64_3d"], default=None,
                     help="profiling case for ncu: the same workload without the relaxation "
                          "prep, --warmup + --steps time steps of one form, no timing output")
     return ap.parse_args()
@@ -595,6 +595,25 @@ def profile_case(args):
     """Small deterministic run for ncu captures (same kernels as the timed leg)."""
     import numpy as np
     import gpue_b200 as G
+    if args.profile.endswith("_3d"):
+        # the 256^3 ground-state workload with the launch shapes the large
+        # leg's autotuner picks on a B200 ((16,16) plan, 2/4/4 lines per CTA),
+        # fixed so that a capture does not depend on timings taken under the
+        # profiler; one step here is one imaginary time step (5 passes)
+        prec = G.PREC_FP32 if args.profile == "fp32_3d" else G.PREC_FP64
+        n = LARGE["n"]
+        with G.Solver(G.make_params(3, n, LARGE["box"], wz=LARGE["wz"], g=LARGE["g"],
+                                    gdt=LARGE["gdt"], precision=prec)) as s:
+            for axis, lines in enumerate((2, 4, 4)):
+                s.set_plan(axis, 16, 0, 0, 16, lines)
+            plans = [s.plan(a) for a in range(3)]
+            s.set_wfc(gauss_start(3, n, LARGE["box"], LARGE["seed"]))
+            r0 = s.evolve(args.warmup, 0)
+            r1 = s.evolve(args.steps, 0, step_offset=args.warmup)
+        print(json.dumps({"profile": args.profile, "warmup_launches": r0["kernel_launches"],
+                          "launches": r1["kernel_launches"], "device_ms": r1["device_ms"],
+                          "plans": plans}))
+        return
     n, box = WORK["n"], WORK["box"]
     dx = box / (n >> 1)
     x = -box + dx * np.arange(n)

@@ -487,8 +487,8 @@ gpue_status gpue_batch_evolve(gpue_batch* b, int32_t gstate, const gpue_batch_op
                                            (o.norm_guard < 0 && c->prec == GPUE_PREC_FP32));
         r.guard[i] = guard;
         BCTX(c, unpolish(c));
-        if (o.autotune) BCTX(c, autotune_ctx(c, c->prec, false));
         BCTX(c, build_tables(c, c->prec, gstate));
+        if (o.autotune) BCTX(c, autotune_ctx(c, c->prec, false));
         BCTX(c, apply_pending_scale(c, c->prec));
         if (guard) {
             BCTX(c, norm_to_slot(c, c->prec, kTargetReal));

@@ -130,7 +130,7 @@ gpue_status build_tables(gpue_ctx* c, int prec, int gstate) {
     if (tb.built_for == gstate) return GPUE_OK;
     const gpue_params& p = c->p;
     auto al = [](size_t b) { return ((b + 255) / 256) * 256; };
-    // per axis: [vfac][kfac] double2, [tw] FP64 complex or FP32 hi then lo,
+    // per axis: [vfac][kfac] double2, [tw] FP64 complex or FP32 (hi, lo) pairs,
     // [pos][mom][vreal] double
     size_t off = 0;
     size_t offs[3][6];
@@ -138,7 +138,7 @@ gpue_status build_tables(gpue_ctx* c, int prec, int gstate) {
         const size_t n = c->ax[a].n;
         offs[a][0] = off; off += al(n * 16);
         offs[a][1] = off; off += al(n * 16);
-        offs[a][2] = off; off += al(n * 16);  // FP64 twiddles, or FP32 hi then lo
+        offs[a][2] = off; off += al(n * 16);  // FP64 twiddles, or FP32 (hi, lo) pairs
         for (int k = 3; k < 6; ++k) { offs[a][k] = off; off += al(n * 8); }
     }
     if (!tb.buf) CK(cudaMalloc(&tb.buf, off));
@@ -166,12 +166,13 @@ gpue_status build_tables(gpue_ctx* c, int prec, int gstate) {
             const long double ang = -2.0L * 3.141592653589793238462643383279L * i / n;
             const double twr = (double)cosl(ang), twi = (double)sinl(ang);
             if (prec == GPUE_PREC_FP32) {
+                // one 16-byte entry per k: the rounded twiddle and its remainder
                 float* tw = (float*)(h.data() + offs[a][2]);
                 const float hr = (float)twr, hi = (float)twi;
-                tw[2 * i] = hr;
-                tw[2 * i + 1] = hi;
-                tw[2 * (n + i)] = (float)(twr - (double)hr);
-                tw[2 * (n + i) + 1] = (float)(twi - (double)hi);
+                tw[4 * i] = hr;
+                tw[4 * i + 1] = hi;
+                tw[4 * i + 2] = (float)(twr - (double)hr);
+                tw[4 * i + 3] = (float)(twi - (double)hi);
             } else {
                 double* tw = (double*)(h.data() + offs[a][2]);
                 tw[2 * i] = twr;
@@ -669,32 +670,39 @@ void destroy_graphs(gpue_ctx* c) {
 
 // Mean device time of one FFT round-trip pass (forward then inverse along
 // the axis) over a copy of the state, with the current launch shape.
-gpue_status time_roundtrip(gpue_ctx* c, int prec, int axis, float* us) {
-    LPass lp;
-    lp.axis = axis;
-    lp.ops = {OP_FFT_F, OP_FFT_I};
-    lp.from_scratch = true;
-    PassArgs a;
-    gpue_status st = make_pass_args(c, prec, lp, 0, a);
+// Device time of a few steps of this context's own schedule (the time kind
+// its tables are built for), so a candidate launch shape is judged by the
+// passes it will run, phases and reductions included.  The state and the
+// scalar slots are saved first and put back after.
+gpue_status time_steps(gpue_ctx* c, int prec, float* us) {
+    const int gstate = c->tab[prec].built_for < 0 ? 0 : c->tab[prec].built_for;
+    gpue_status st = build_tables(c, prec, gstate);
     if (st) return st;
-    a.active = nullptr;
-    const LaunchCfg& lc = c->lc[prec][axis];
-    void (*fn)(PassArgs) = axis == 0 ? lc.k->row : lc.k->col;
-    // unnormalised round trips grow the values by n per launch: 8 launches
-    // stay far inside the FP32 range for n <= 1024
-    CK(cudaMemcpyAsync(c->scratch, state_of(c, prec), c->N * elem_size(prec),
-                       cudaMemcpyDeviceToDevice, c->stream));
-    for (int w = 0; w < 2; ++w)
-        CK(launch_kernel(fn, lc.blocks, lc.threads, lc.smem, c->stream, false, a));
-    const int reps = 6;
+    if (!c->have_wfc)  // any finite state times the same; this one is ~1e-2 (FP32)
+        CK(cudaMemsetAsync(state_of(c, prec), 0x3C, c->N * elem_size(prec), c->stream));
+    const int nsteps = 4, reps = 2;
+    double saved[kNScal];
+    const size_t bytes = c->N * elem_size(prec);
+    CK(cudaMemcpyAsync(c->scratch, state_of(c, prec), bytes, cudaMemcpyDeviceToDevice,
+                       c->stream));
+    CK(cudaMemcpyAsync(saved, c->scal, sizeof saved, cudaMemcpyDeviceToHost, c->stream));
+    const std::vector<double> rexp;
+    const long launches = c->launches;
+    st = enqueue_steps(c, prec, 0, nsteps, gstate, false, rexp, false, false);
+    if (st) return st;
     CK(cudaEventRecord(c->ev0, c->stream));
-    for (int r = 0; r < reps; ++r)
-        CK(launch_kernel(fn, lc.blocks, lc.threads, lc.smem, c->stream, false, a));
+    for (int r = 0; r < reps && !st; ++r)
+        st = enqueue_steps(c, prec, 0, nsteps, gstate, false, rexp, false, false);
+    if (st) return st;
     CK(cudaEventRecord(c->ev1, c->stream));
-    CK(cudaEventSynchronize(c->ev1));
+    CK(cudaMemcpyAsync(state_of(c, prec), c->scratch, bytes, cudaMemcpyDeviceToDevice,
+                       c->stream));
+    CK(cudaMemcpyAsync(c->scal, saved, sizeof saved, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->launches = launches;
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
-    *us = ms * 1e3f / reps;
+    *us = ms * 1e3f / (reps * nsteps);
     return GPUE_OK;
 }
 
@@ -714,7 +722,7 @@ gpue_status autotune_ctx(gpue_ctx* c, int prec, bool force) {
             return fail(c, GPUE_ERR_CUDA, "no launch shape for length %d", c->ax[axis].n);
         c->lc[prec][axis] = def;
         float def_us = 0.f;
-        gpue_status st = time_roundtrip(c, prec, axis, &def_us);
+        gpue_status st = time_steps(c, prec, &def_us);
         if (st) return st;
         LaunchCfg best = def;
         float best_us = def_us;
@@ -725,8 +733,8 @@ gpue_status autotune_ctx(gpue_ctx* c, int prec, bool force) {
                 if (cand.k == def.k && cand.lines == def.lines) continue;
                 c->lc[prec][axis] = cand;
                 float t0 = 0.f, t1 = 0.f;
-                st = time_roundtrip(c, prec, axis, &t0);
-                if (!st) st = time_roundtrip(c, prec, axis, &t1);
+                st = time_steps(c, prec, &t0);
+                if (!st) st = time_steps(c, prec, &t1);
                 if (st) return st;
                 const float t = std::min(t0, t1);
                 if (t < 0.97f * best_us) {  // a clear gain only: noise must not flip plans

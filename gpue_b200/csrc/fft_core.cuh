@@ -261,8 +261,8 @@ struct LineFFT {
         static constexpr int G = N / (R * P);
         static constexpr int step = N / (Ns * R);
         static constexpr int NQ = (S > 0 && P % Ns == 0) ? 1 : G;
-        // complex64 twiddles come as hi/lo pairs (the table holds N hi values
-        // and then N lo values)
+        // complex64 twiddles come as hi/lo pairs: entry k of the table is one
+        // 16-byte (hi.x, hi.y, lo.x, lo.y), read with a single load
         static constexpr bool SPLIT = kSplitTwiddles && std::is_same<T, float>::value;
         static constexpr int WPER = SPLIT ? 2 : 1;
         static constexpr bool HOLD = NQ * (R - 1) * WPER <= 16;
@@ -278,9 +278,16 @@ struct LineFFT {
                 for (int q = 0; q < NQ; ++q) {
                     const int jm = (t + P * q) % Ns;
 #pragma unroll
-                    for (int r = 1; r < R; ++r)
-#pragma unroll
-                        for (int h = 0; h < WPER; ++h) w[q][r - 1][h] = tw[h * N + jm * r * step];
+                    for (int r = 1; r < R; ++r) {
+                        const int k = jm * r * step;
+                        if constexpr (SPLIT) {
+                            const float4 e = __ldg(reinterpret_cast<const float4*>(tw) + k);
+                            w[q][r - 1][0] = cx<T>{e.x, e.y};
+                            w[q][r - 1][WPER - 1] = cx<T>{e.z, e.w};
+                        } else {
+                            w[q][r - 1][0] = tw[k];
+                        }
+                    }
                 }
             }
         }
@@ -291,8 +298,12 @@ struct LineFFT {
                 else return cmul(a, w[qq][r - 1][0]);
             } else {
                 const int k = ((t + P * q) % Ns) * r * step;
-                if constexpr (SPLIT) return cmul_split(a, tw[k], tw[N + k]);
-                else return cmul(a, tw[k]);
+                if constexpr (SPLIT) {
+                    const float4 e = __ldg(reinterpret_cast<const float4*>(tw) + k);
+                    return cmul_split(a, cx<float>{e.x, e.y}, cx<float>{e.z, e.w});
+                } else {
+                    return cmul(a, tw[k]);
+                }
             }
         }
     };

@@ -88,7 +88,7 @@ struct PassArgs {
     const double2* kfac[3];  // per-axis kinetic factor (FP64)
     const double* pos[3];
     const double* mom[3];
-    const void* tw;  // cx<T>[N]: W_N^k for this axis
+    const void* tw;  // W_N^k for this axis: cx<double>[N], or (hi, lo) float pairs [N]
     RedArgs red;
     const double* scale_in;   // OP_SCALE factor
     const double* kscale_in;  // optional extra OP_KPHASE factor (real-time norm guard)
@@ -577,15 +577,20 @@ __device__ __forceinline__ KSum pass_tiles(const PassArgs& a, long t0, long tste
                     }
                     break;
                 }
+                // The thread's E terms are summed in plain FP64 (relative
+                // error ~E * 2^-53) and enter the compensated sum once per tile.
                 case OP_NORM: {
+                    double part = 0.0;
 #pragma unroll
                     for (int e = 0; e < E; ++e) {
                         const double re = (double)v[e].x, im = (double)v[e].y;
-                        acc.add(re * re + im * im);
+                        part += re * re + im * im;
                     }
+                    acc.add(part);
                     break;
                 }
                 case OP_EKIN: {
+                    double part = 0.0;
 #pragma unroll
                     for (int e = 0; e < E; ++e) {
                         const int k = L::index(t, e);
@@ -594,8 +599,9 @@ __device__ __forceinline__ KSum pass_tiles(const PassArgs& a, long t0, long tste
                         const double pz = a.mom[2][a.axis == 2 ? k : zi];
                         const double K = a.kin_coef * (px * px + py * py + pz * pz);
                         const double re = (double)v[e].x, im = (double)v[e].y;
-                        acc.add(K * (re * re + im * im));
+                        part += K * (re * re + im * im);
                     }
+                    acc.add(part);
                     break;
                 }
                 default:

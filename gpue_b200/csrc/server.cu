@@ -179,8 +179,8 @@ gpue_status start_solve(gpue_server* S, const Pending& p, Solve& s) {
     s.steps = 0;
     s.guard = p.req.gstate == 1 && c->prec == GPUE_PREC_FP32;
     st = gpue_set_wfc(c, p.req.psi0, GPUE_MEM_HOST, GPUE_C128);
-    if (!st && S->o.autotune) st = autotune_ctx(c, c->prec, false);
     if (!st) st = build_tables(c, c->prec, p.req.gstate);
+    if (!st && S->o.autotune) st = autotune_ctx(c, c->prec, false);
     if (!st && s.guard) {
         st = norm_to_slot(c, c->prec, kTargetReal);
         if (!st && cudaMemcpyAsync(c->scal + kGuard, c->scal + kOne, sizeof(double),

@@ -276,9 +276,10 @@ gpue_status gpue_ctx_wfc_device(gpue_ctx* ctx, void** psi, int32_t* dtype);
 /* No counterpart in GPUE (which hands its transforms to cuFFT plans,
  * src/ds.cu:11-79): choose, by timing on this device, the FFT radix plan and
  * the lines per CTA of every axis of the context's grid.  Each compiled plan
- * of the axis length and each lines-per-CTA count that fits is timed on a
- * forward/inverse round trip over a copy of the state; the fastest (by a
- * clear margin over the default) is kept.  Choices are cached per (precision,
+ * of the axis length and each lines-per-CTA count that fits is timed on four
+ * time steps of the context's own schedule (the time kind its operators are
+ * built for, imaginary if none), run on the state and then undone; the
+ * fastest (by a clear margin over the default) is kept.  Choices are cached per (precision,
  * dimension, length, axis) for the process, so later contexts of the same
  * shape reuse them without timing; flags bit 0 re-times a cached shape.
  * Setting GPUE_AUTOTUNE=1 in the environment makes gpue_ctx_create do this. */
@@ -291,7 +292,7 @@ typedef struct gpue_plan_info {
     int32_t lines_per_cta;
     int32_t threads, blocks;       /* CTA size and persistent grid */
     int32_t tuned;                 /* 1 if chosen by gpue_autotune */
-    float us, default_us;          /* round-trip pass times measured by the tuner */
+    float us, default_us;          /* step times (us) the tuner measured: chosen, default */
 } gpue_plan_info;
 
 /* The launch shape the context uses along an axis (0 = x). */
