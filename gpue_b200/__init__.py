@@ -178,6 +178,7 @@ def lib():
         L.gpue_energy.argtypes = [vp, C.POINTER(C.c_double)]
         L.gpue_norm.argtypes = [vp, C.POINTER(C.c_double)]
         L.gpue_observables_get.argtypes = [vp, C.POINTER(Observables)]
+        L.gpue_set_check_observables.argtypes = [vp, C.POINTER(Observables), i32]
         L.gpue_find_vortices.argtypes = [vp, C.c_double, vp, i32, vp, i32, C.POINTER(i32)]
         L.gpue_ctx_stream.argtypes = [vp, C.POINTER(vp)]
         L.gpue_ctx_wfc_device.argtypes = [vp, C.POINTER(vp), C.POINTER(i32)]
@@ -221,7 +222,8 @@ def lib():
                      "gpue_batch_destroy", "gpue_batch_evolve", "gpue_autotune",
                      "gpue_get_plan", "gpue_set_gauge_tables", "gpue_observables_get",
                      "gpue_find_vortices", "gpue_set_potential_table", "gpue_snapshot_save",
-                     "gpue_snapshot_load", "gpue_list_plans", "gpue_set_plan"):
+                     "gpue_snapshot_load", "gpue_list_plans", "gpue_set_plan",
+                     "gpue_set_check_observables"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -375,6 +377,16 @@ class Solver:
                                           MEM_HOST, lst.ctypes.data_as(vp) if cap else None,
                                           cap, C.byref(found)))
         return marker, lst[:min(found.value, cap)], found.value
+
+    def record_check_observables(self, cap):
+        """Record observables at every energy check of later evolve calls
+        (gpue_set_check_observables); cap = 0 turns it off."""
+        self._obs_buf = (Observables * max(int(cap), 1))() if cap else None
+        self._ck(lib().gpue_set_check_observables(self._h, self._obs_buf, int(cap)))
+
+    def check_observables(self, n):
+        """The observables of the first n checks of the latest evolve call."""
+        return [self._obs_buf[k].as_dict() for k in range(n)]
 
     def observables(self):
         """Energy terms, trapezoid density moments and <L_z> of the current

@@ -126,6 +126,8 @@ struct ObsArgs {
     double2* partials;  // [kObsN][gridDim.x]
     unsigned* counter;  // zero between launches; reset by the last CTA
     double* out;        // [kObsN]
+    double* ereal;      // optional: potential + interaction + rotation sums (energy_calc's
+                        // real-space part, as k_energy_real leaves it)
 };
 
 __device__ __forceinline__ double trapz_w(int i, int n) {
@@ -204,6 +206,7 @@ __global__ void __launch_bounds__(256) k_observables(const ObsArgs o) {
     __syncthreads();
     if (!s_last) return;
     __threadfence();
+    __shared__ double fin[kObsN];
     if (threadIdx.x < kObsN) {
         const int q = threadIdx.x;
         KSum t{0.0, 0.0};
@@ -211,9 +214,14 @@ __global__ void __launch_bounds__(256) k_observables(const ObsArgs o) {
             const double2 p = __ldcg(o.partials + (long)q * gridDim.x + i);
             t.merge(p.x, p.y);
         }
-        o.out[q] = t.s + t.c;
+        fin[q] = t.s + t.c;
+        o.out[q] = fin[q];
     }
-    if (threadIdx.x == 0) *o.counter = 0u;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (o.ereal) *o.ereal = fin[kObsPot] + fin[kObsInt] + fin[kObsRot];
+        *o.counter = 0u;
+    }
 }
 
 // Energy check of batched solves, one block.  flags[2] counts a solve's

@@ -545,11 +545,52 @@ gpue_status launch_energy(gpue_ctx* c, int prec, int gstate, bool scale_pending,
         pdl = true;
     }
     EnergyArgs e = energy_args(c, prec, scale_pending);
-    const int blocks = c->sms * 4;
-    if (prec == GPUE_PREC_FP32) k_energy_real<float><<<blocks, 256, 0, c->stream>>>(e);
-    else k_energy_real<double><<<blocks, 256, 0, c->stream>>>(e);
+    if (c->obs_out) {
+        // the observables reduction in place of the real-space energy pass:
+        // one read of psi, energy_calc's real-space sum left in kEreal
+        ObsArgs oa;
+        std::memset(&oa, 0, sizeof oa);
+        oa.e = e;
+        oa.partials = e.red.partials;
+        oa.counter = e.red.counter;
+        oa.out = c->obs_dev;
+        oa.ereal = c->scal + kEreal;
+        const int blocks = (int)std::min<long>(c->sms * 2, (kAuxPartials - kObsN) / kObsN);
+        if (prec == GPUE_PREC_FP32) k_observables<float><<<blocks, 256, 0, c->stream>>>(oa);
+        else k_observables<double><<<blocks, 256, 0, c->stream>>>(oa);
+    } else {
+        const int blocks = c->sms * 4;
+        if (prec == GPUE_PREC_FP32) k_energy_real<float><<<blocks, 256, 0, c->stream>>>(e);
+        else k_energy_real<double><<<blocks, 256, 0, c->stream>>>(e);
+    }
     c->launches++;
     CK(cudaGetLastError());
+    return GPUE_OK;
+}
+
+// The observables of the latest energy check (launch_energy with obs_out set)
+// into the caller's array entry k, scaled as gpue_observables_get scales them.
+gpue_status read_check_observables(gpue_ctx* c, int k) {
+    if (!c->obs_out || k >= c->obs_cap) return GPUE_OK;
+    double h[kObsN], ekin;
+    CK(cudaMemcpyAsync(h, c->obs_dev, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(&ekin, c->scal + kEkin, sizeof ekin, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    gpue_observables& o = c->obs_out[k];
+    std::memset(&o, 0, sizeof o);
+    const double dV = c->dV;
+    o.norm = h[kObsNorm] * dV;
+    o.e_kinetic = ekin / (double)c->N * dV;
+    o.e_potential = h[kObsPot] * dV;
+    o.e_interaction = h[kObsInt] * dV;
+    o.e_rotation = h[kObsRot] * dV;
+    o.energy = o.e_kinetic + o.e_potential + o.e_interaction + o.e_rotation;
+    o.x = h[kObsX] * dV;
+    o.y = h[kObsY] * dV;
+    o.z = h[kObsZ] * dV;
+    o.r2 = h[kObsR2] * dV;
+    o.q = h[kObsQ] * dV;
+    o.lz = h[kObsLz] * dV;
     return GPUE_OK;
 }
 
@@ -633,7 +674,7 @@ gpue_status run_segment(gpue_ctx* c, int prec, int i0, int i1, int gstate, bool 
     if (!rexp.empty() || c->time_dep)
         return enqueue_steps(c, prec, i0, i1, gstate, scale_first, rexp, energy_after, guard);
     GraphKey key{prec, gstate, i0 % 2, i1 - i0, scale_first ? 1 : 0, energy_after ? 1 : 0,
-                 guard ? 1 : 0};
+                 guard ? 1 : 0, c->obs_out ? 1 : 0};
     auto it = c->graphs.find(key);
     if (it == c->graphs.end()) {
         const long before = c->launches;
@@ -810,6 +851,7 @@ gpue_status step_loop(gpue_ctx* c, int prec, int off, int nsteps, int gstate,
         if (check) {
             double energy;
             st = read_energy(c, &energy);
+            if (!st) st = read_check_observables(c, lo.n_en);
             if (st) return st;
             lo.energy = energy;
             lo.n_en++;
@@ -1009,6 +1051,7 @@ gpue_status gpue_ctx_destroy(gpue_ctx* c) {
         if (t) cudaFree(t);
     if (c->progs) cudaFree(c->progs);
     if (c->vtx_ws) cudaFree(c->vtx_ws);
+    if (c->obs_dev) cudaFree(c->obs_dev);
     cudaFree(c->scratch);
     cudaFree(c->scal);
     cudaFree(c->partials);
@@ -1139,6 +1182,17 @@ gpue_status gpue_observables_get(gpue_ctx* c, gpue_observables* o) {
     o->r2 = h[kObsR2] * dV;
     o->q = h[kObsQ] * dV;
     o->lz = h[kObsLz] * dV;
+    return GPUE_OK;
+}
+
+gpue_status gpue_set_check_observables(gpue_ctx* c, gpue_observables* out, int32_t cap) {
+    if (!c || cap < 0 || (cap > 0 && !out)) return GPUE_ERR_INVALID_ARG;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    if (cap > 0 && !c->obs_dev) CK(cudaMalloc(&c->obs_dev, kObsN * sizeof(double)));
+    c->obs_out = cap > 0 ? out : nullptr;
+    c->obs_cap = cap;
+    destroy_graphs(c);  // captured checks hold the other reduction
     return GPUE_OK;
 }
 

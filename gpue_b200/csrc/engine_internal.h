@@ -58,7 +58,7 @@ struct LaunchCfg {
 };
 
 struct GraphKey {
-    int prec, gstate, parity, nsteps, scale_first, energy_last, guard;
+    int prec, gstate, parity, nsteps, scale_first, energy_last, guard, observables;
     bool operator<(const GraphKey& o) const {
         return std::memcmp(this, &o, sizeof(GraphKey)) < 0;
     }
@@ -110,6 +110,10 @@ struct gpue_ctx {
     int prog_off[5] = {-1, -1, -1, -1, -1};  // V, k, Ax, Ay, Az
     int prog_len[5] = {};
     bool time_dep = false;     // some factor is evaluated per step
+    // gpue_set_check_observables: observables at every energy check
+    gpue_observables* obs_out = nullptr;  // caller's array, obs_cap entries
+    int obs_cap = 0;
+    double* obs_dev = nullptr;            // the reduction's kObsN results
     void* vtx_ws = nullptr;    // gpue_find_vortices workspace (allocated on first use)
     size_t vtx_ws_bytes = 0;
 };

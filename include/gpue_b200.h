@@ -184,6 +184,16 @@ typedef struct gpue_observables {
 
 gpue_status gpue_observables_get(gpue_ctx* ctx, gpue_observables* out);
 
+/* Observables at the energy checks of gpue_evolve (the survey's "fused into
+ * the check passes"): with an array set, every check runs the observables
+ * reduction in place of energy_calc's real-space pass (one read of psi
+ * either way; the energy it leaves is energy_calc's, summed per term) and
+ * check k of each gpue_evolve call (k counted from 0; gpue_evolve_result
+ * .n_energies of them) is stored in out[k] for k < cap.  out must stay valid
+ * while it is set; NULL / 0 turns recording off.  Single contexts only: the
+ * batch and server paths keep the plain energy check. */
+gpue_status gpue_set_check_observables(gpue_ctx* ctx, gpue_observables* out, int32_t cap);
+
 /* Binary snapshots for checkpoint and resume (GPUE only has the text dumps of
  * FileIO::writeOut/readIn, src/fileIO.cu:13-72, restarted with -r).  A
  * snapshot holds the state exactly as the context keeps it (the precision it

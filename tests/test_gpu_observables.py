@@ -170,3 +170,35 @@ def test_single_vortex_angular_momentum_sign(charge):
     obs, _, _, back = run(c, 0, 0, psi0=psi)
     assert obs["lz"] == pytest.approx(charge, abs=0.05)
     check_against_numpy(c, obs, back, 1e-11)
+
+
+@pytest.mark.parametrize("gs", [0, 1])
+def test_observables_recorded_at_energy_checks(gs):
+    """gpue_set_check_observables: every check of an evolve call yields the
+    observables of the state it checks (those gpue_observables_get gives for
+    that state), without changing the run."""
+    import gpue_b200 as G
+    c = case(dim=2, n=128, box=8.0, g=200.0, omega=0.5, gauge=True, dt=5e-5)
+    psi0 = cases.initial_psi(c)
+    with G.Solver(product_params(c, G.PREC_FP64)) as s:
+        s.set_wfc(psi0)
+        plain = s.evolve(400, gs, energy_every=100)
+        want_psi = s.get_wfc()
+    with G.Solver(product_params(c, G.PREC_FP64)) as s:
+        s.record_check_observables(8)
+        s.set_wfc(psi0)
+        r = s.evolve(400, gs, energy_every=100)
+        got_psi = s.get_wfc()
+        rec = s.check_observables(r["n_energies"])
+    assert r["n_energies"] == plain["n_energies"] == 4
+    assert np.array_equal(got_psi, want_psi)
+    assert r["energy"] == pytest.approx(plain["energy"], rel=1e-13)
+    assert rec[-1]["energy"] == pytest.approx(r["energy"], rel=1e-13)
+    # the check at step 300 sees the state after 301 steps
+    with G.Solver(product_params(c, G.PREC_FP64)) as s:
+        s.set_wfc(psi0)
+        s.evolve(301, gs)
+        ref = s.observables()
+    for k in ref:
+        assert rec[3][k] == pytest.approx(ref[k], rel=1e-12, abs=1e-15), k
+    assert rec[0]["norm"] > 0 and len({round(o["lz"], 12) for o in rec}) > 1
