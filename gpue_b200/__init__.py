@@ -146,7 +146,8 @@ class ServerStats(C.Structure):
                 ("bytes_resident", C.c_int64), ("bytes_peak", C.c_int64),
                 ("bytes_budget", C.c_int64), ("ticks", C.c_int64),
                 ("kernel_launches", C.c_int64), ("point_steps", C.c_double),
-                ("busy_s", C.c_double)]
+                ("busy_s", C.c_double), ("admit_s", C.c_double), ("issue_s", C.c_double),
+                ("finish_s", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

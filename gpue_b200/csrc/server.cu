@@ -103,9 +103,22 @@ struct Run {
     // this tick
     std::vector<int> members;  // indices into the active list
     bool issued = false;
+    // The last tick captured as a graph, replayed while the run's solves
+    // (and the parity of their step counts) stay the same: a tick's kernel
+    // arguments then do not change, so neither planning nor upload is needed.
+    cudaGraphExec_t exec = nullptr;
+    std::vector<std::pair<uint64_t, int>> exec_key;  // (solve serial, step parity)
+    long exec_launches = 0;
+    void drop_graph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        exec_key.clear();
+        exec_launches = 0;
+    }
 };
 
 struct Solve {
+    uint64_t serial = 0;  // unique per admitted request (context addresses get reused)
     gpue_ctx* c = nullptr;
     gpue_request req{};
     double t_submit = 0, t_admit = 0;
@@ -135,6 +148,7 @@ struct gpue_server {
     std::string err;                       // guarded by mu
     std::vector<Solve> active;             // worker only
     Run run[2];                            // worker only
+    uint64_t next_serial = 1;              // worker only
 };
 
 namespace {
@@ -235,6 +249,7 @@ void admit(gpue_server* S) {
         if (S->st.bytes_resident > S->st.bytes_peak) S->st.bytes_peak = S->st.bytes_resident;
         S->st.admitted++;
         S->st.active++;
+        s.serial = S->next_serial++;
         S->active.push_back(s);
     }
 }
@@ -244,6 +259,22 @@ gpue_status issue_run(gpue_server* S, int gstate, Run& R, long& launches, std::s
     R.issued = false;
     if (R.members.empty()) return GPUE_OK;
     const int n = (int)R.members.size();
+    std::vector<std::pair<uint64_t, int>> key;
+    key.reserve(n);
+    for (int m : R.members) key.emplace_back(S->active[m].serial, S->active[m].steps % 2);
+    if (R.exec && key == R.exec_key) {
+        cudaEventRecord(R.e0, R.stream);
+        cudaError_t e = cudaGraphLaunch(R.exec, R.stream);
+        cudaEventRecord(R.e1, R.stream);
+        if (e != cudaSuccess) {
+            err = std::string("tick replay: ") + cudaGetErrorString(e);
+            return GPUE_ERR_CUDA;
+        }
+        launches += R.exec_launches;
+        R.issued = true;
+        return GPUE_OK;
+    }
+    R.drop_graph();
     BatchRun r;
     r.gstate = gstate;
     r.every = S->o.check_steps;
@@ -307,19 +338,37 @@ gpue_status issue_run(gpue_server* S, int gstate, Run& R, long& launches, std::s
         err = "tick argument upload";
         return GPUE_ERR_CUDA;
     }
+    // capture the tick (launches, gather, result copy) and launch the graph
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(R.stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        enqueue_segment(plan, r, R.stream, R.lanes, static_cast<const CheckArgs*>(checks),
+                        R.nactive);
+        k_batch_gather<<<(n + 127) / 128, 128, 0, R.stream>>>(
+            static_cast<const CheckArgs*>(checks), n, R.outs);
+        cudaMemcpyAsync(R.h_outs, R.outs, n * sizeof(BatchOut), cudaMemcpyDeviceToHost,
+                        R.stream);
+        const cudaError_t le = cudaGetLastError();
+        e = cudaStreamEndCapture(R.stream, &g);
+        if (e == cudaSuccess) e = le;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&R.exec, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        R.exec = nullptr;
+        err = std::string("tick capture: ") + cudaGetErrorString(e);
+        return GPUE_ERR_CUDA;
+    }
+    R.exec_key = std::move(key);
+    R.exec_launches = plan.launches + 1;
     cudaEventRecord(R.e0, R.stream);
-    enqueue_segment(plan, r, R.stream, R.lanes, static_cast<const CheckArgs*>(checks),
-                    R.nactive);
-    k_batch_gather<<<(n + 127) / 128, 128, 0, R.stream>>>(static_cast<const CheckArgs*>(checks),
-                                                           n, R.outs);
-    cudaMemcpyAsync(R.h_outs, R.outs, n * sizeof(BatchOut), cudaMemcpyDeviceToHost, R.stream);
+    e = cudaGraphLaunch(R.exec, R.stream);
     cudaEventRecord(R.e1, R.stream);
-    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         err = std::string("tick launch: ") + cudaGetErrorString(e);
         return GPUE_ERR_CUDA;
     }
-    launches += plan.launches + 1;
+    launches += R.exec_launches;
     R.issued = true;
     return GPUE_OK;
 }
@@ -352,10 +401,13 @@ gpue_status tick(gpue_server* S, std::string& err) {
     for (size_t i = 0; i < S->active.size(); ++i)
         S->run[S->active[i].req.gstate].members.push_back((int)i);
     long launches = 0;
+    const auto ti = std::chrono::steady_clock::now();
     for (int g = 0; g < 2; ++g) {
         gpue_status st = issue_run(S, g, S->run[g], launches, err);
         if (st) return st;
     }
+    const double issue_s =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - ti).count();
     double busy = 0, pts = 0;
     const Run* first = nullptr;  // the runs overlap: time from the first start
     for (int g = 0; g < 2; ++g) {
@@ -371,6 +423,7 @@ gpue_status tick(gpue_server* S, std::string& err) {
         busy = std::max(busy, (double)ms * 1e-3);
     }
     std::vector<char> leave(S->active.size(), 0);
+    const auto tf = std::chrono::steady_clock::now();
     for (int g = 0; g < 2; ++g) {
         Run& R = S->run[g];
         if (!R.issued) continue;
@@ -383,6 +436,7 @@ gpue_status tick(gpue_server* S, std::string& err) {
             if (stopped || s.steps >= s.req.max_steps) {
                 finish(S, s, bo, stopped);
                 leave[R.members[k]] = 1;
+                R.drop_graph();  // its arguments name the context just freed
             }
         }
     }
@@ -390,7 +444,11 @@ gpue_status tick(gpue_server* S, std::string& err) {
     for (size_t i = 0; i < S->active.size(); ++i)
         if (!leave[i]) keep.push_back(S->active[i]);
     S->active.swap(keep);
+    const double finish_s =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - tf).count();
     std::lock_guard<std::mutex> lk(S->mu);
+    S->st.issue_s += issue_s;
+    S->st.finish_s += finish_s;
     S->st.ticks++;
     S->st.kernel_launches += launches;
     S->st.point_steps += pts;
@@ -408,7 +466,14 @@ void worker_main(gpue_server* S) {
                                     [&] { return S->stop || !S->queue.empty(); });
             if (S->stop) return;
         }
+        const auto ta = std::chrono::steady_clock::now();
         admit(S);
+        {
+            const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() -
+                                                            ta).count();
+            std::lock_guard<std::mutex> lk(S->mu);
+            S->st.admit_s += dt;
+        }
         if (S->active.empty()) continue;
         std::string err;
         gpue_status st = tick(S, err);
@@ -490,6 +555,7 @@ gpue_status gpue_server_destroy(gpue_server* S) {
         if (s.c) gpue_ctx_destroy(s.c);
     for (Run& R : S->run) {
         if (R.stream) cudaStreamSynchronize(R.stream);
+        R.drop_graph();
         R.lanes.destroy();
         R.sink.release();
         if (R.outs) cudaFree(R.outs);

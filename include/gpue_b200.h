@@ -431,6 +431,9 @@ typedef struct gpue_server_stats {
     int64_t ticks, kernel_launches;
     double point_steps;  /* grid points x steps run by all ticks */
     double busy_s;       /* device time of the ticks (CUDA events) */
+    double admit_s;      /* worker's host time admitting solves (context set-up) */
+    double issue_s;      /* worker's host time planning and enqueuing ticks */
+    double finish_s;     /* worker's host time returning finished solves */
 } gpue_server_stats;
 
 gpue_status gpue_server_create(const gpue_server_opts* opts, gpue_server** out);
