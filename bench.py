@@ -463,9 +463,11 @@ def serve_leg(G, dev):
     reqs = serve_requests(G)
     psi0 = [gauss_start(q["dim"], q["n"], q["box"], q["seed"]) for q in reqs]
     results = {}
+    # default plans: timing every fresh shape of the burst before its first
+    # tick costs more (~0.6 s) than the tuned plans save over a 2000-step solve
     with G.Server(precision=G.PREC_FP32, check_steps=SERVE["check"], threshold=SERVE["thr"],
                   threshold_abs=True, hbm_budget=SERVE["budget"], device=dev,
-                  autotune=True) as srv:
+                  autotune=False) as srv:
         t0 = time.perf_counter()
 
         def submitter():

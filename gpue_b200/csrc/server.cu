@@ -178,8 +178,10 @@ gpue_server_result make_result(const gpue_request& q, gpue_status status, double
     return r;
 }
 
-// Context of an admitted request, ready for its first tick.
-gpue_status start_solve(gpue_server* S, const Pending& p, Solve& s) {
+// Context of an admitted request, ready for its first tick.  With tune
+// false (admission while a tick runs) no plans are timed: contention would
+// skew them; shapes tuned before still get their cached choices.
+gpue_status start_solve(gpue_server* S, const Pending& p, Solve& s, bool tune) {
     gpue_params prm = p.req.params;
     prm.precision = S->o.precision;
     prm.device = S->o.device;
@@ -194,7 +196,7 @@ gpue_status start_solve(gpue_server* S, const Pending& p, Solve& s) {
     s.guard = p.req.gstate == 1 && c->prec == GPUE_PREC_FP32;
     st = gpue_set_wfc(c, p.req.psi0, GPUE_MEM_HOST, GPUE_C128);
     if (!st) st = build_tables(c, c->prec, p.req.gstate);
-    if (!st && S->o.autotune) st = autotune_ctx(c, c->prec, false);
+    if (!st && S->o.autotune && tune) st = autotune_ctx(c, c->prec, false);
     if (!st && s.guard) {
         st = norm_to_slot(c, c->prec, kTargetReal);
         if (!st && cudaMemcpyAsync(c->scal + kGuard, c->scal + kOne, sizeof(double),
@@ -210,7 +212,7 @@ gpue_status start_solve(gpue_server* S, const Pending& p, Solve& s) {
     return st;
 }
 
-void admit(gpue_server* S) {
+void admit(gpue_server* S, bool tune) {
     for (;;) {
         Pending p;
         size_t est = 0;
@@ -235,7 +237,7 @@ void admit(gpue_server* S) {
             S->st.bytes_resident += (int64_t)est;  // reserved until the context exists
         }
         Solve s;
-        gpue_status st = start_solve(S, p, s);
+        gpue_status st = start_solve(S, p, s, tune);
         std::lock_guard<std::mutex> lk(S->mu);
         S->st.bytes_resident -= (int64_t)est;
         if (st) {
@@ -396,11 +398,13 @@ void finish(gpue_server* S, Solve& s, const BatchOut& bo, bool stopped) {
     push_result(S, r);
 }
 
-gpue_status tick(gpue_server* S, std::string& err) {
+// Enqueues one tick of every resident solve (both runs); returns without
+// waiting for the device.
+gpue_status tick_issue(gpue_server* S, long& launches, std::string& err) {
     for (int g = 0; g < 2; ++g) S->run[g].members.clear();
     for (size_t i = 0; i < S->active.size(); ++i)
         S->run[S->active[i].req.gstate].members.push_back((int)i);
-    long launches = 0;
+    launches = 0;
     const auto ti = std::chrono::steady_clock::now();
     for (int g = 0; g < 2; ++g) {
         gpue_status st = issue_run(S, g, S->run[g], launches, err);
@@ -408,6 +412,14 @@ gpue_status tick(gpue_server* S, std::string& err) {
     }
     const double issue_s =
         std::chrono::duration<double>(std::chrono::steady_clock::now() - ti).count();
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->st.issue_s += issue_s;
+    return GPUE_OK;
+}
+
+// Waits for the issued tick and retires the solves that are done.  Solves
+// admitted meanwhile (appended to the active list) took no part in it.
+gpue_status tick_complete(gpue_server* S, long launches, std::string& err) {
     double busy = 0, pts = 0;
     const Run* first = nullptr;  // the runs overlap: time from the first start
     for (int g = 0; g < 2; ++g) {
@@ -447,7 +459,6 @@ gpue_status tick(gpue_server* S, std::string& err) {
     const double finish_s =
         std::chrono::duration<double>(std::chrono::steady_clock::now() - tf).count();
     std::lock_guard<std::mutex> lk(S->mu);
-    S->st.issue_s += issue_s;
     S->st.finish_s += finish_s;
     S->st.ticks++;
     S->st.kernel_launches += launches;
@@ -466,19 +477,26 @@ void worker_main(gpue_server* S) {
                                     [&] { return S->stop || !S->queue.empty(); });
             if (S->stop) return;
         }
-        const auto ta = std::chrono::steady_clock::now();
-        admit(S);
-        {
+        auto timed_admit = [&](bool tune) {
+            const auto ta = std::chrono::steady_clock::now();
+            admit(S, tune);
             const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() -
                                                             ta).count();
             std::lock_guard<std::mutex> lk(S->mu);
             S->st.admit_s += dt;
-        }
+        };
+        timed_admit(true);
         if (S->active.empty()) continue;
         std::string err;
-        gpue_status st = tick(S, err);
+        long launches = 0;
+        gpue_status st = tick_issue(S, launches, err);
+        // requests that arrived meanwhile are set up while the device works
+        if (!st) timed_admit(false);
+        if (!st) st = tick_complete(S, launches, err);
         if (st) {
-            // the device state of every resident solve is now unknown
+            // the device state of every resident solve is now unknown; let
+            // whatever was enqueued drain before the contexts are freed
+            cudaDeviceSynchronize();
             for (Solve& s : S->active) {
                 push_result(S, make_result(s.req, st, s.t_submit, s.t_admit, now_s(S)));
                 gpue_ctx_destroy(s.c);
