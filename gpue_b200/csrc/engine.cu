@@ -212,7 +212,8 @@ bool build_cfg(gpue_ctx* c, int prec, int axis, const PassKernel* k, int C, Laun
     int max_smem = 48 * 1024;
     cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
     if (smem > (size_t)max_smem) return false;
-    void* fns[4] = {(void*)k->row, (void*)k->col, (void*)k->row_batch, (void*)k->col_batch};
+    void* fns[6] = {(void*)k->row,       (void*)k->col,     (void*)k->row_batch,
+                    (void*)k->col_batch, (void*)k->row_ext, (void*)k->col_ext};
     if (smem > 48 * 1024)
         for (void* f : fns)
             if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
