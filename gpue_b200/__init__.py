@@ -55,7 +55,7 @@ class EvolveOpts(C.Structure):
                 ("threshold_abs", C.c_int32), ("polish_steps", C.c_int32),
                 ("graph_chunk", C.c_int32), ("no_sync", C.c_int32),
                 ("step_offset", C.c_int32), ("norm_guard", C.c_int32),
-                ("reserved", C.c_int32 * 4)]
+                ("norm_guard_period", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 class EvolveResult(C.Structure):
@@ -341,9 +341,11 @@ class Solver:
         self._ck(lib().gpue_get_wfc(self._h, C.c_void_p(ptr), MEM_DEVICE, dtype))
 
     def evolve(self, nsteps, gstate, energy_every=0, threshold=-1.0, threshold_abs=False,
-               polish_steps=0, graph_chunk=0, no_sync=False, step_offset=0, norm_guard=-1):
+               polish_steps=0, graph_chunk=0, no_sync=False, step_offset=0, norm_guard=-1,
+               norm_guard_period=0):
         o = EvolveOpts()
         o.norm_guard = norm_guard
+        o.norm_guard_period = norm_guard_period
         o.no_sync = 1 if no_sync else 0
         o.step_offset = step_offset
         o.energy_calc_steps = energy_every

@@ -198,7 +198,7 @@ gpue_status plan_axis(gpue_ctx* c, int prec, int axis);
 // and keeps the fastest for each axis (cached per shape for the process).
 gpue_status autotune_ctx(gpue_ctx* c, int prec, bool force);
 gpue_status make_pass_args(gpue_ctx* c, int prec, const LPass& lp, int gstate, PassArgs& a);
-void step_passes(gpue_ctx* c, int i, int gstate, bool scale_first, double rexp, bool guard,
+void step_passes(gpue_ctx* c, int i, int gstate, bool scale_first, double rexp, int guard,
                  std::vector<LPass>& out);
 void fuse(std::vector<LPass>& v);
 std::vector<LPass> energy_passes(const gpue_ctx* c, bool scale_pending);

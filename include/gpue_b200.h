@@ -100,7 +100,10 @@ typedef struct gpue_evolve_opts {
     int32_t norm_guard;            /* real time only: rescale to the starting norm each
                                       step (a no-op in exact arithmetic); -1 = on for
                                       the FP32 form, off for FP64; 0 off; 1 on */
-    int32_t reserved[4];
+    int32_t norm_guard_period;     /* guard every 1, 2 or 4 steps; 0 = default (2): the
+                                      factor of a step's norm scales the next step's
+                                      kinetic phase */
+    int32_t reserved[3];
 } gpue_evolve_opts;
 
 typedef struct gpue_evolve_result {
