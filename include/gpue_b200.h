@@ -205,7 +205,9 @@ gpue_status gpue_set_check_observables(gpue_ctx* ctx, gpue_observables* out, int
  * gpue_params it belongs to, the caller's phase and step, and a checksum.
  * Loading it into a context with the same parameters (precision and device
  * may differ) and continuing with gpue_evolve's step_offset = step repeats
- * the uninterrupted run bit for bit in the same precision.  Field tables and
+ * the uninterrupted run bit for bit in the same precision, except with the
+ * real-time norm guard (on by default for FP32), which every gpue_evolve call
+ * starts afresh from the norm it finds: then to FP32 round-off.  Field tables and
  * parameter-file fields are not part of a snapshot: install them again.
  * Saves write "<path>.tmp" and rename it over path.  Load fails with
  * GPUE_ERR_INVALID_ARG for another grid or parameters, a bad header, a short
