@@ -34,13 +34,14 @@ CASES = {
     # 3D imaginary time with the gauge
     "g3d_imag_gauge_n32": dict(dim=3, n=32, box=6.0, wz=2.0, g=100.0, omega=0.3, gauge=True,
                                gsteps=100, seed=17, init="gauss", energy_every=50),
-    # 256^2, g=100, gdt=1e-4, 10000 imaginary steps
+    # the 256^2 imaginary-time workload: g=100, gdt=1e-4, 10000 steps
     "cfg1_256_imag": dict(dim=2, n=256, box=10.0, g=100.0, gsteps=10000, seed=1,
                           init="gauss", energy_every=1000),
 }
 
-# Full-size configurations timed on GPUE's own build (make_golden.py --timing):
-# configs[0..2] shapes with the step counts used for timing.
+# Full-size workloads timed on GPUE's own build (make_golden.py --timing): the
+# 1024^2 rotating real-time case and the 256^3 ground state, with the step
+# counts used for timing.
 CASES.update({
     "cfg2_1024_real_gauge": dict(dim=2, n=1024, box=16.0, g=500.0, omega=0.7, gauge=True,
                                  dt=5e-5, esteps=20000, seed=2, init="phase"),
