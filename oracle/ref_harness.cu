@@ -16,6 +16,7 @@
 // Usage (key=value):
 //   gpue_ref_harness dim=2 n=64 box=10 wx=1 wy=1 wz=1 gamma=1 g=100 gpe=1
 //       omega=0 gauge=0 gdt=1e-4 dt=1e-4 gsteps=100 esteps=0 energy_every=0
+//       [ramp=1 ramp_type=1]
 //       psi0=in.bin out=prefix data=/tmp/dir
 // Writes prefix_imag.bin / prefix_real.bin (complex128, x fastest, hbar=m=1
 // units) and prefix_imag.txt / prefix_real.txt ("energy <E>" and
@@ -144,6 +145,10 @@ int main(int argc, char** argv) {
         a.push_back("-l");
         a.push_back("-w");
         a.push_back(fmt(getd("omega", 0)));
+    }
+    if (geti("ramp", 0)) {  // parseArgs' -R <ramp_type> (src/parser.cu:188-194)
+        a.push_back("-R");
+        a.push_back(std::to_string(geti("ramp_type", 1)));
     }
     std::vector<char*> av;
     for (auto& s : a) av.push_back(const_cast<char*>(s.c_str()));

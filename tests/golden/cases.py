@@ -34,6 +34,14 @@ CASES = {
     # 3D imaginary time with the gauge
     "g3d_imag_gauge_n32": dict(dim=3, n=32, box=6.0, wz=2.0, g=100.0, omega=0.3, gauge=True,
                                gsteps=100, seed=17, init="gauss", energy_every=50),
+    # 2D imaginary time with GPUE's gauge ramp (-R 1 and -R 2): the gauge
+    # factors raised to a cumulative power every step
+    "g2d_imag_ramp1_n64": dict(dim=2, n=64, box=8.0, g=200.0, omega=0.5, gauge=True,
+                               gdt=2e-4, gsteps=150, seed=18, init="gauss", energy_every=50,
+                               ramp=True, ramp_type=1),
+    "g2d_imag_ramp2_n64": dict(dim=2, n=64, box=8.0, g=150.0, omega=0.6, gauge=True,
+                               gdt=2e-4, gsteps=120, seed=19, init="gauss", energy_every=40,
+                               ramp=True, ramp_type=2),
     # the 256^2 imaginary-time workload: g=100, gdt=1e-4, 10000 steps
     "cfg1_256_imag": dict(dim=2, n=256, box=10.0, g=100.0, gsteps=10000, seed=1,
                           init="gauss", energy_every=1000),
@@ -52,7 +60,7 @@ TIMING = [("cfg1_256_imag", 10000), ("cfg2_1024_real_gauge", 1000), ("cfg3_256_i
 FIXTURES = [k for k in CASES if not k.startswith(("cfg2", "cfg3"))]
 
 DEFAULTS = dict(wx=1.0, wy=1.0, wz=1.0, gamma=1.0, g=0.0, gpe=True, omega=0.0, gauge=False,
-                gdt=1e-4, dt=1e-4, gsteps=0, esteps=0, energy_every=0)
+                gdt=1e-4, dt=1e-4, gsteps=0, esteps=0, energy_every=0, ramp=False, ramp_type=1)
 
 
 def case(name):
@@ -99,6 +107,7 @@ def harness_args(c, psi0_path, out_prefix, data_dir):
          "gpe=%d" % int(c["gpe"]), "omega=%r" % c["omega"], "gauge=%d" % int(c["gauge"]),
          "gdt=%r" % c["gdt"], "dt=%r" % c["dt"], "gsteps=%d" % c["gsteps"],
          "esteps=%d" % c["esteps"], "energy_every=%d" % c["energy_every"],
+         "ramp=%d" % int(c["ramp"]), "ramp_type=%d" % c["ramp_type"],
          "psi0=" + psi0_path, "out=" + out_prefix, "data=" + data_dir]
     return a
 

@@ -31,14 +31,16 @@ def oracle_problem(c, **kw):
     return oracle.Problem(c["dim"], c["n"], c["box"], wx=c["wx"], wy=c["wy"], wz=c["wz"],
                           gamma=c["gamma"], g=c["g"], gpe=c["gpe"], omega=c["omega"],
                           gauge=c["gauge"], gdt=c["gdt"], dt=c["dt"],
-                          energy_every=c["energy_every"], **kw)
+                          energy_every=c["energy_every"], ramp=c.get("ramp", False),
+                          ramp_type=c.get("ramp_type", 1), **kw)
 
 
 def product_params(c, precision):
     import gpue_b200 as G
     return G.make_params(c["dim"], c["n"], c["box"], wx=c["wx"], wy=c["wy"], wz=c["wz"],
                          gamma=c["gamma"], g=c["g"], gpe=c["gpe"], omega=c["omega"],
-                         gauge=c["gauge"], gdt=c["gdt"], dt=c["dt"], precision=precision)
+                         gauge=c["gauge"], gdt=c["gdt"], dt=c["dt"], precision=precision,
+                         ramp=c.get("ramp", False), ramp_type=c.get("ramp_type", 1))
 
 
 def run_product(c, precision, psi0=None, **evolve_kw):
