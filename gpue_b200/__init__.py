@@ -189,6 +189,10 @@ def lib():
                                            C.POINTER(C.c_double), i32]
         L.gpue_ast_parse.argtypes = [C.c_char_p, C.POINTER(C.c_char_p), C.POINTER(C.c_double),
                                      i32, vp, i32, C.POINTER(i32)]
+        L.gpue_ast_parse_file.argtypes = [C.c_char_p, C.POINTER(C.c_char_p),
+                                          C.POINTER(C.c_double), i32, i32, C.c_char_p, i32,
+                                          C.POINTER(i32), vp, i32, C.POINTER(i32),
+                                          C.POINTER(i32)]
         L.gpue_batch_create.argtypes = [C.POINTER(vp), i32, C.POINTER(vp)]
         L.gpue_batch_destroy.argtypes = [vp]
         L.gpue_batch_last_error.argtypes = [vp]
@@ -219,7 +223,8 @@ def lib():
         for name in ("gpue_default_params", "gpue_ctx_create", "gpue_ctx_destroy",
                      "gpue_set_operators", "gpue_set_wfc", "gpue_get_wfc", "gpue_evolve",
                      "gpue_energy", "gpue_norm", "gpue_ctx_stream", "gpue_ctx_wfc_device",
-                     "gpue_load_param_text", "gpue_ast_parse", "gpue_batch_create",
+                     "gpue_load_param_text", "gpue_ast_parse", "gpue_ast_parse_file",
+                     "gpue_batch_create",
                      "gpue_batch_destroy", "gpue_batch_evolve", "gpue_autotune",
                      "gpue_get_plan", "gpue_set_gauge_tables", "gpue_observables_get",
                      "gpue_find_vortices", "gpue_set_potential_table", "gpue_snapshot_save",

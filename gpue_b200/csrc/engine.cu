@@ -1391,6 +1391,37 @@ gpue_status gpue_ast_parse(const char* expr, const char* const* names, const dou
     return GPUE_OK;
 }
 
+gpue_status gpue_ast_parse_file(const char* text, const char* const* names,
+                                const double* values, int32_t nvalues, int32_t entry,
+                                char* name, int32_t name_cap, int32_t* time_flag,
+                                void* nodes_out, int32_t cap, int32_t* count,
+                                int32_t* nentries) {
+    if (!text || !count || !nentries || cap < 0 || nvalues < 0 || entry < 0)
+        return GPUE_ERR_INVALID_ARG;
+    std::map<std::string, double> m;
+    for (int i = 0; i < nvalues; ++i)
+        if (names && names[i] && values) m[names[i]] = values[i];
+    std::map<std::string, AstExpr> asts;
+    std::vector<std::string> order;
+    std::string err;
+    if (!ast_parse_file(text, m, asts, order, err)) return GPUE_ERR_AST;
+    *nentries = (int32_t)order.size();
+    if (entry >= (int32_t)order.size()) return GPUE_ERR_INVALID_ARG;
+    const std::string& nm = order[entry];
+    const AstExpr& e = asts[nm];
+    *count = (int32_t)e.nodes.size();
+    if (time_flag) *time_flag = e.time_dependent ? 1 : 0;
+    if (name) {
+        if (name_cap <= (int32_t)nm.size()) return GPUE_ERR_INVALID_ARG;
+        std::memcpy(name, nm.c_str(), nm.size() + 1);
+    }
+    if (nodes_out && cap >= *count)
+        std::memcpy(nodes_out, e.nodes.data(), e.nodes.size() * sizeof(AstNode));
+    else if (nodes_out)
+        return GPUE_ERR_INVALID_ARG;
+    return GPUE_OK;
+}
+
 gpue_status gpue_ctx_wfc_device(gpue_ctx* c, void** psi, int32_t* dtype) {
     if (!c || !psi || !dtype) return GPUE_ERR_INVALID_ARG;
     *psi = c->psi;

@@ -11,17 +11,18 @@
 // library holds until the process exits.
 //
 // The array's name is only a host-side stand-in in host code; the device
-// address comes from cudaGetSymbolAddress, taken once per device (with that
-// device current) the first time the entry point runs there.  Every call on a
-// device shares the one array and it keeps the previous call's contents: the
-// arrival counter is cleared before each launch, and calls whose kernels
-// overlap on the GPU (different streams, no ordering between them) race on
-// the array.
+// address comes from cudaGetSymbolAddress, asked on every call with the
+// caller's device current (a lookup that allocates nothing), so a device
+// whose primary context was reset in between gets its new address.  The
+// first call on a device also loads the library's device code there, so make
+// it before any stream capture.  Every call on a device shares the one array
+// and it keeps the previous call's contents: the arrival counter is cleared
+// before each launch, and calls whose kernels overlap on the GPU (different
+// streams, no ordering between them) race on the array.
 
 #include <cuda_runtime.h>
 
 #include <cstdio>
-#include <mutex>
 
 #include "../../include/gpue_b200.h"
 #include "pass.cuh"
@@ -44,10 +45,6 @@ struct NaScratch {
 constexpr size_t kNaBytes = sizeof(NaScratch);
 
 static __device__ __align__(256) NaScratch g_na_scratch;
-
-constexpr int kNaMaxDevices = 64;
-std::mutex g_na_mu;
-NaScratch* g_na_ptr[kNaMaxDevices] = {};
 
 // This entry point has no context to hold a message, so failures are reported
 // by the status code and one line on stderr.
@@ -109,21 +106,10 @@ extern "C" gpue_status gpue_norm_noalloc(const void* psi, int32_t dtype, int64_t
                  (long long)npoints, kNaMaxPoints, kNaBytes);
         return na_fail(GPUE_ERR_INVALID_ARG, m);
     }
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNaMaxDevices)
-        return na_fail(GPUE_ERR_CUDA, "gpue_norm_noalloc: no usable current device");
-    NaScratch* sp = nullptr;
-    {
-        std::lock_guard<std::mutex> lk(g_na_mu);
-        if (!g_na_ptr[dev]) {
-            void* p = nullptr;
-            cudaError_t e = cudaGetSymbolAddress(&p, g_na_scratch);
-            if (e != cudaSuccess || !p)
-                return na_fail(GPUE_ERR_CUDA, "gpue_norm_noalloc: cudaGetSymbolAddress failed");
-            g_na_ptr[dev] = static_cast<NaScratch*>(p);
-        }
-        sp = g_na_ptr[dev];
-    }
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_na_scratch) != cudaSuccess || !p)
+        return na_fail(GPUE_ERR_CUDA, "gpue_norm_noalloc: cudaGetSymbolAddress failed");
+    NaScratch* sp = static_cast<NaScratch*>(p);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (cudaMemsetAsync(&sp->counter, 0, sizeof(unsigned), s) != cudaSuccess)
         return na_fail(GPUE_ERR_CUDA, "gpue_norm_noalloc: clearing the counter failed");

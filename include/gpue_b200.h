@@ -268,6 +268,21 @@ gpue_status gpue_load_param_text(gpue_ctx* ctx, const char* text, int32_t time_m
 gpue_status gpue_ast_parse(const char* expr, const char* const* names, const double* values,
                            int32_t nvalues, void* nodes_out, int32_t cap, int32_t* count);
 
+/* parse_param_file's host part (src/dynamic.cu:162-222, with parse_eqn and
+ * tree_to_array, src/dynamic.cu:227-507) on the text of a parameter file:
+ * entry `entry` (0-based, in file order) as GPUE's flat EqnNode_gpu array, as
+ * allocate_eqn builds it before its device copy.  *nentries receives the number
+ * of entries, `name` (name_cap bytes) the entry's name, *time_flag GPUE's
+ * "<name>_time" flag (the entry uses t or names an earlier entry).  Lines
+ * without '=' continue the previous entry and V gets
+ * +0.5*mass*(Ax*Ax+Ay*Ay+Az*Az) unless it is the last entry.  nodes_out may be
+ * NULL to query the sizes; no device work. */
+gpue_status gpue_ast_parse_file(const char* text, const char* const* names,
+                                const double* values, int32_t nvalues, int32_t entry,
+                                char* name, int32_t name_cap, int32_t* time_flag,
+                                void* nodes_out, int32_t cap, int32_t* count,
+                                int32_t* nentries);
+
 /* GPUE's file gauge (-A file: file_A and generate_gauge, src/operators.cu:259-270,
  * 505-520): full-field Ax, Ay, Az (host arrays of xDim*yDim*zDim doubles, x
  * fastest, already multiplied by omega as file_A does; NULL for a zero
@@ -333,10 +348,12 @@ gpue_status gpue_set_plan(gpue_ctx* ctx, int32_t axis, int32_t ra, int32_t rb, i
  * nothing here: the reduction scratch is a fixed 1 MiB device array that
  * every GPU loading the library holds until exit, which caps npoints at
  * 2^28 (larger sizes return GPUE_ERR_INVALID_ARG with a message on stderr).
- * Asynchronous on `stream` (a cudaStream_t, may be NULL).  The first call on
- * a device looks up the array's device address; make that first call before
- * any stream capture.  All calls share the array, so calls whose kernels can
- * overlap on the GPU race; order them on one stream.  dtype is GPUE_C128 or
+ * Asynchronous on `stream` (a cudaStream_t, may be NULL).  Every call looks
+ * up the array's device address on the current device (a lookup, no
+ * allocation); the first call on a device also loads the library's device code
+ * there, so make that first call before any stream capture.  All calls share
+ * the array, so calls whose kernels can overlap on the GPU race; order them on
+ * one stream.  dtype is GPUE_C128 or
  * GPUE_C64. */
 gpue_status gpue_norm_noalloc(const void* psi, int32_t dtype, int64_t npoints, double dV,
                               double* out, void* stream);

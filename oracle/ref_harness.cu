@@ -27,17 +27,35 @@
 // the n x n complex128 state in psi0 with GPUE's x grid, and writes the marker
 // array (int32, n*n) to prefix_vortex.bin and "found <count>" to
 // prefix_vortex.txt.  This mode makes no CUDA call and needs no GPU.
+//
+//   gpue_ref_harness mode=ast doubles=names.txt exprs=exprs.txt out=prefix
+//   gpue_ref_harness mode=ast doubles=names.txt param=file.cfg out=prefix
+// runs only GPUE's host-side equation parser (parse_eqn, find_element_num and
+// tree_to_array, src/dynamic.cu:227-530) with a Grid holding the doubles of
+// names.txt ("name value" lines).  With exprs, every line is one expression
+// parsed as entry "V"; with param, the file is read line by line as
+// parse_param_file does (src/dynamic.cu:187-222: spaces dropped, lines without
+// '=' continue the previous entry, V gets +0.5*mass*(Ax*Ax+Ay*Ay+Az*Az) unless
+// it is the last entry) and each entry goes through allocate_eqn's host part
+// (src/dynamic.cu:162-185; the device copy is left out).  prefix_ast.txt gets,
+// per entry, "entry <name> <count> <time_flag>" and then one line per
+// EqnNode_gpu: "<val as %a> <is_dynamic> <var> <left> <right> <op_num>", with
+// op_num written as 0 for leaves (GPUE leaves it unset there).  No CUDA call.
 
+#include <algorithm>
+#include <cctype>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <fstream>
 #include <map>
 #include <string>
 #include <vector>
 
 #include "constants.h"
 #include "ds.h"
+#include "dynamic.h"
 #include "evolution.h"
 #include "init.h"
 #include "parser.h"
@@ -82,6 +100,66 @@ void dump(Grid& par, const std::string& path, int gsize, double L, int dim, doub
     fclose(t);
 }
 
+void ast_entry(Grid& par, FILE* out, const std::string& name, const std::string& expr) {
+    par.store(name + "_time", false);
+    EqnNode tree = parse_eqn(par, expr, name);
+    int num = 0;
+    find_element_num(tree, num);
+    std::vector<EqnNode_gpu> arr(num);
+    int count = 0;
+    tree_to_array(tree, arr.data(), count);
+    par.store(name, tree);
+    fprintf(out, "entry %s %d %d\n", name.c_str(), num, par.bval(name + "_time") ? 1 : 0);
+    for (const EqnNode_gpu& e : arr)
+        fprintf(out, "%a %d %d %d %d %d\n", e.val, e.is_dynamic ? 1 : 0, (int)e.var, e.left,
+                e.right, e.left >= 0 ? e.op_num : 0);
+}
+
+int ast_mode() {
+    Grid par;
+    {
+        FILE* f = fopen(get("doubles", "doubles.txt").c_str(), "r");
+        if (!f) {
+            fprintf(stderr, "cannot read doubles\n");
+            return 2;
+        }
+        char name[256];
+        double v;
+        while (fscanf(f, "%255s %lf", name, &v) == 2) par.store(std::string(name), v);
+        fclose(f);
+    }
+    FILE* out = fopen((get("out", "ref") + "_ast.txt").c_str(), "w");
+    const std::string param = get("param", "");
+    if (!param.empty()) {
+        std::ifstream file(param);
+        std::string line, val_string, eqn_string;
+        while (std::getline(file, line)) {
+            line.erase(std::remove_if(line.begin(), line.end(), ::isspace), line.end());
+            const size_t it = line.find('=');
+            if (it == std::string::npos) {
+                eqn_string += line;
+            } else {
+                if (!val_string.empty()) {
+                    if (val_string == "V") eqn_string += "+0.5*mass*(Ax*Ax+Ay*Ay+Az*Az)";
+                    ast_entry(par, out, val_string, eqn_string);
+                    val_string.clear();
+                    eqn_string.clear();
+                }
+                val_string = line.substr(0, it);
+                eqn_string = line.substr(it + 1);
+            }
+        }
+        ast_entry(par, out, val_string, eqn_string);
+    } else {
+        std::ifstream file(get("exprs", "exprs.txt"));
+        std::string line;
+        while (std::getline(file, line))
+            if (!line.empty()) ast_entry(par, out, "V", line);
+    }
+    fclose(out);
+    return 0;
+}
+
 int vortex_mode() {
     const int n = geti("n", 64);
     const double xMax = getd("box", 10);
@@ -121,6 +199,7 @@ int main(int argc, char** argv) {
         if (eq != std::string::npos) g_kv[a.substr(0, eq)] = a.substr(eq + 1);
     }
     if (get("mode", "") == "vortex") return vortex_mode();
+    if (get("mode", "") == "ast") return ast_mode();
     const int dim = geti("dim", 2);
     const int n = geti("n", 64);
     const int gsteps = geti("gsteps", 0), esteps = geti("esteps", 0);

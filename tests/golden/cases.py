@@ -57,6 +57,8 @@ CASES.update({
                           init="gauss"),
 })
 TIMING = [("cfg1_256_imag", 10000), ("cfg2_1024_real_gauge", 1000), ("cfg3_256_imag", 100)]
+# Full-size runs kept as digests (make_golden.py --digest) with their step counts.
+DIGESTS = {"cfg2_1024_real_gauge": 1000, "cfg3_256_imag": 100}
 FIXTURES = [k for k in CASES if not k.startswith(("cfg2", "cfg3"))]
 
 DEFAULTS = dict(wx=1.0, wy=1.0, wz=1.0, gamma=1.0, g=0.0, gpe=True, omega=0.0, gauge=False,
@@ -164,3 +166,52 @@ def vortex_psi(v):
 def vortex_harness_args(v, psi0_path, out_prefix):
     return ["mode=vortex", "n=%d" % v["n"], "box=%r" % v["box"], "radius=%r" % v["radius"],
             "psi0=" + psi0_path, "out=" + out_prefix]
+
+
+# Equation-AST inputs pinned to GPUE's own parser (make_golden.py --ast runs
+# the harness's host-only mode=ast on them and stores ast_gpue.json).  The
+# doubles stand for Grid values the expressions may name.
+AST_DOUBLES = {"omega": 0.7, "omegaX": 1.25, "omegaY": 0.8, "mass": 2.0, "xMax": 10.0,
+               "fudge": 0.0, "rad": 10.0, "omegaR": 7071.0}
+
+AST_CORPUS = [
+    "(((3*x)+7)+(5-7)+cos(0)*1)+pow(120,2)",
+    "x-y-z",
+    "x-y+z",
+    "2*x-3",
+    "x/y*z",
+    "x^2",
+    "pow(x,3)+pow(y,2)",
+    "exp(0-x)",
+    "sqrt(x*x+y*y)",
+    "cos(omega*t)*x",
+    "0.5*mass*((omegaX*x)*(omegaX*x)+(omegaY*y)*(omegaY*y))",
+    "rad*omegaR*x*y*z",
+    "((x))",
+    "(x+1)*(y-2)",
+    "sin(x)*cos(y)+tan(z)",
+    "jn(0,x)+yn(1,y)",
+    "1.5+2.25*x",
+    "[x+y]*2",
+    "x*y*omega*omegaX*30000",
+    "((3*x)+(y-(2*z)))/(1+t)",
+    "k2n(2,x)",
+    "exp(0-t)*sqrt(x)",
+]
+# Expressions GPUE's parse_eqn rejects (it prints "No value ... found!" and
+# exits): a two-argument function nested inside another function's argument.
+AST_REJECTED = ["sqrt(pow(x,2)+pow(y,2))", "sqrt(pow(x,2))"]
+
+# Parameter-file texts: parse_param_file's line rules (continuations, the
+# m|A|^2/2 suffix on V unless it is last, entries naming earlier entries).
+AST_PARAM_TEXTS = {
+    "rotation_gauge": "Ax = 0-y*omega\nAy = x*omega\nAz = 0\nV = 0.5*(x*x+y*y)\nK = 1\n",
+    "continued_lines": ("Ax = 0\nAy = 0\nAz = 0\nV = 0.5*mass*\n(omegaX*omegaX*x*x\n"
+                        "+omegaY*omegaY*y*y)\nK = cos(omega*t)\n"),
+    "time_gauge": ("Ax = 0-y*omega*cos(omega*t)\nAy = x*omega\nAz = 0\n"
+                   "V = 0.5*(x*x+y*y)\nK = 1\n"),
+    "named_entries": "w = 2\nAx = 0\nAy = 0\nAz = 0\nV = w*w*x*x\nK = x\n",
+}
+# GPUE's own parameter files, read from the reference checkout when the
+# fixture is made and stored in it with their parse.
+AST_REFERENCE_FILES = ["src/example.cfg", "src/gauge.cfg"]

@@ -1,40 +1,25 @@
-"""GPUE's equation grammar: the library's C++ parser against the oracle's
-restatement (oracle/ast_oracle.py), node for node, and GPUE's own
+"""GPUE's equation grammar: the library's C++ parser and the oracle's
+restatement (oracle/ast_oracle.py) against GPUE's own parser, node for node
+(tests/golden/ast_gpue.json: parse_eqn, find_element_num and tree_to_array of
+src/dynamic.cu:162-530, run host-only by the harness's mode=ast on the corpus,
+on parameter texts and on GPUE's example parameter files), and GPUE's own
 dynamic_test known answer (src/unit_test.cu:396-466).  CPU only."""
 import ctypes as C
+import json
 import math
+import os
 
 import numpy as np
 import pytest
 
 import ast_oracle
+import cases
 import oracle
 
-DOUBLES = {"omega": 0.7, "omegaX": 1.25, "omegaY": 0.8, "mass": 2.0, "xMax": 10.0,
-           "fudge": 0.0, "rad": 10.0, "omegaR": 7071.0}
-
-CORPUS = [
-    "(((3*x)+7)+(5-7)+cos(0)*1)+pow(120,2)",
-    "a-b-c".replace("a", "x").replace("b", "y").replace("c", "z"),
-    "x-y+z",
-    "2*x-3",
-    "x/y*z",
-    "x^2",
-    "pow(x,3)+pow(y,2)",
-    "exp(-x)".replace("-x", "0-x"),
-    "sqrt(x*x+y*y)",
-    "cos(omega*t)*x",
-    "0.5*mass*((omegaX*x)*(omegaX*x)+(omegaY*y)*(omegaY*y))",
-    "rad*omegaR*x*y*z",
-    "((x))",
-    "(x+1)*(y-2)",
-    "sin(x)*cos(y)+tan(z)",
-    "jn(0,x)+yn(1,y)",
-    "1.5+2.25*x",
-    "[x+y]*2",
-    "x*y*omega*omegaX*30000",
-    "((3*x)+(y-(2*z)))/(1+t)",
-]
+DOUBLES = cases.AST_DOUBLES
+CORPUS = cases.AST_CORPUS
+GPUE_AST = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                       "ast_gpue.json")))
 
 
 def lib():
@@ -106,3 +91,83 @@ def test_param_file_restatement_appends_gauge_energy_to_V():
     ax, ay = -3.0 * 0.7, 2.0 * 0.7
     assert val == pytest.approx(0.5 * 13 + 0.5 * 2.0 * (ax * ax + ay * ay), rel=1e-15)
     assert "V" in flags  # it names earlier expressions, so GPUE marks it time dependent
+
+
+def same_nodes(got, gpue_nodes):
+    """Node for node: value bit for bit, flags, links; op_num where GPUE sets it
+    (tree_to_array copies an unset op_num for leaves, written as 0)."""
+    assert len(got) == len(gpue_nodes)
+    for a, b in zip(got, gpue_nodes):
+        a = list(a)
+        assert a[0] == b[0] and [int(v) for v in a[1:5]] == b[1:5], (a, b)
+        if b[3] >= 0:
+            assert int(a[5]) == b[5], (a, b)
+
+
+def product_file_entries(text, doubles=DOUBLES):
+    L = lib()
+    names = (C.c_char_p * len(doubles))(*[k.encode() for k in doubles])
+    vals = (C.c_double * len(doubles))(*doubles.values())
+    cnt, nent, tf = C.c_int32(), C.c_int32(), C.c_int32()
+    st = L.gpue_ast_parse_file(text.encode(), names, vals, len(doubles), 0, None, 0, None,
+                               None, 0, C.byref(cnt), C.byref(nent))
+    if st != 0:
+        return st, None
+    out = []
+    for i in range(nent.value):
+        name = C.create_string_buffer(64)
+        st = L.gpue_ast_parse_file(text.encode(), names, vals, len(doubles), i, name, 64,
+                                   C.byref(tf), None, 0, C.byref(cnt), C.byref(nent))
+        assert st == 0
+        buf = (oracle.Node * cnt.value)()
+        st = L.gpue_ast_parse_file(text.encode(), names, vals, len(doubles), i, name, 64,
+                                   C.byref(tf), C.cast(buf, C.c_void_p), cnt.value,
+                                   C.byref(cnt), C.byref(nent))
+        assert st == 0
+        out.append((name.value.decode(), tf.value,
+                    [(n.val, n.is_dynamic, n.var, n.left, n.right, n.op_num) for n in buf]))
+    return 0, out
+
+
+def test_fixture_covers_the_corpus():
+    assert [c["expr"] for c in GPUE_AST["corpus"]] == CORPUS
+    assert GPUE_AST["doubles"] == DOUBLES
+
+
+@pytest.mark.parametrize("k", range(len(CORPUS)))
+def test_parser_matches_gpue(k):
+    ref = GPUE_AST["corpus"][k]
+    st, nodes = product_nodes(ref["expr"])
+    assert st == 0
+    same_nodes(nodes, ref["nodes"])
+    same_nodes(ast_oracle.tree_to_array(ast_oracle.parse_eqn(ref["expr"], DOUBLES, {})),
+               ref["nodes"])
+    # GPUE's "<name>_time" flag, through a one-entry parameter text
+    st, entries = product_file_entries("V = " + ref["expr"])
+    assert st == 0 and len(entries) == 1
+    assert entries[0][1] == ref["time"]
+    same_nodes(entries[0][2], ref["nodes"])
+
+
+@pytest.mark.parametrize("k", range(len(GPUE_AST["param_files"])),
+                         ids=[p["name"] for p in GPUE_AST["param_files"]])
+def test_param_file_matches_gpue(k):
+    pf = GPUE_AST["param_files"][k]
+    st, entries = product_file_entries(pf["text"])
+    assert st == 0
+    assert [e[0] for e in entries] == [e["name"] for e in pf["entries"]]
+    asts, order, flags = ast_oracle.parse_param_text(pf["text"], DOUBLES)
+    assert order == [e["name"] for e in pf["entries"]]
+    for (name, tflag, nodes), ref in zip(entries, pf["entries"]):
+        assert tflag == ref["time"], name
+        same_nodes(nodes, ref["nodes"])
+        same_nodes(ast_oracle.tree_to_array(asts[name]), ref["nodes"])
+        assert (name in flags) == bool(ref["time"]), name
+
+
+@pytest.mark.parametrize("k", range(len(cases.AST_REJECTED)))
+def test_rejects_what_gpue_rejects(k):
+    ref = GPUE_AST["rejected"][k]
+    assert ref["exit_code"] != 0  # GPUE printed its message and exited
+    st, _ = product_nodes(ref["expr"])
+    assert st == 5

@@ -20,14 +20,22 @@ from helpers import product_params
 pytestmark = pytest.mark.gpu
 
 
+# One block (64^2 = 4096 points), and several blocks with a ragged last one
+# (96^2 = 2.25 blocks, 160^2 = 6.25 blocks) or whole ones (32^3 = 8 blocks), so
+# the cross-block merge, the counter reset and the tail bounds check all run.
+SHAPES = [(2, 64), (2, 96), (2, 160), (3, 32)]
+
+
 @pytest.mark.parametrize("precision", [0, 1])
-def test_norm_noalloc_matches_gpue_norm_twice(precision):
+@pytest.mark.parametrize("shape", SHAPES, ids=["%dd-%d" % s for s in SHAPES])
+def test_norm_noalloc_matches_gpue_norm_twice(precision, shape):
     import torch
 
     import gpue_b200 as G
-    c = cases.case("g2d_real_gauge_n64")
+    dim, n = shape
+    c = dict(cases.DEFAULTS, dim=dim, n=n, box=8.0, seed=70 + n, init="phase")
     psi0 = cases.initial_psi(c) * 1.7  # a norm away from 1
-    dV = (c["box"] / (c["n"] >> 1)) ** 2
+    dV = (c["box"] / (c["n"] >> 1)) ** dim
     with G.Solver(product_params(c, precision)) as s:
         s.set_wfc(psi0)
         ref = s.norm()
