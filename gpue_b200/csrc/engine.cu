@@ -131,18 +131,31 @@ gpue_status build_tables(gpue_ctx* c, int prec, int gstate) {
     const gpue_params& p = c->p;
     auto al = [](size_t b) { return ((b + 255) / 256) * 256; };
     // per axis: [vfac][kfac] double2, [tw] FP64 complex or FP32 (hi, lo) pairs,
-    // [pos][mom][vreal] double
+    // [pos][mom][vreal] double, [vd][kd] float2
     size_t off = 0;
-    size_t offs[3][6];
+    size_t offs[3][8];
     for (int a = 0; a < 3; ++a) {
         const size_t n = c->ax[a].n;
         offs[a][0] = off; off += al(n * 16);
         offs[a][1] = off; off += al(n * 16);
         offs[a][2] = off; off += al(n * 16);  // FP64 twiddles, or FP32 (hi, lo) pairs
         for (int k = 3; k < 6; ++k) { offs[a][k] = off; off += al(n * 8); }
+        for (int k = 6; k < 8; ++k) { offs[a][k] = off; off += al(n * 8); }
     }
     if (!tb.buf) CK(cudaMalloc(&tb.buf, off));
     std::vector<unsigned char> h(off, 0);
+    // factor - 1 of exp(-a) (imaginary time) or exp(-i a) (real time), formed
+    // without cancellation in long double and rounded once to FP32
+    auto fdelta = [&](long double ang, float* d) {
+        if (gstate == 0) {
+            d[0] = (float)expm1l(-ang);
+            d[1] = 0.f;
+        } else {
+            const long double h = sinl(0.5L * ang);
+            d[0] = (float)(-2.0L * h * h);
+            d[1] = (float)(-sinl(ang));
+        }
+    };
     for (int a = 0; a < 3; ++a) {
         const Axis& A = c->ax[a];
         const int n = A.n;
@@ -150,8 +163,13 @@ gpue_status build_tables(gpue_ctx* c, int prec, int gstate) {
         axis_potential(c, a, va);
         double* vf = (double*)(h.data() + offs[a][0]);
         double* kf = (double*)(h.data() + offs[a][1]);
+        float* vd = (float*)(h.data() + offs[a][6]);
+        float* kd = (float*)(h.data() + offs[a][7]);
         for (int i = 0; i < n; ++i) {
             const double K = (p.hbar * p.hbar / (2 * p.mass)) * (A.p[i] * A.p[i]);
+            const double Dt = gstate == 0 ? p.gdt : p.dt;
+            fdelta((long double)va[i] * ((long double)Dt / (2.0L * p.hbar)), vd + 2 * i);
+            fdelta((long double)K * ((long double)Dt / p.hbar), kd + 2 * i);
             if (gstate == 0) {
                 vf[2 * i] = std::exp(-va[i] * (p.gdt / (2 * p.hbar)));
                 vf[2 * i + 1] = 0.0;
@@ -193,6 +211,8 @@ gpue_status build_tables(gpue_ctx* c, int prec, int gstate) {
         tb.pos[a] = (const double*)(b + offs[a][3]);
         tb.mom[a] = (const double*)(b + offs[a][4]);
         tb.vreal[a] = (const double*)(b + offs[a][5]);
+        tb.vd[a] = (const float2*)(b + offs[a][6]);
+        tb.kd[a] = (const float2*)(b + offs[a][7]);
     }
     tb.built_for = gstate;
     return GPUE_OK;
@@ -296,12 +316,59 @@ gpue_status plan_axis(gpue_ctx* c, int prec, int axis) {
     return GPUE_OK;
 }
 
+gpue_status plan_plane(gpue_ctx* c, int prec) {
+    PlaneCfg& pc = c->plane[prec];
+    pc = PlaneCfg();
+    const char* env = std::getenv("GPUE_PLANE");
+    if (env && env[0] == '0') return GPUE_OK;
+    if (c->dim != 3 || c->ax[0].n != c->ax[1].n) return GPUE_OK;
+    const PlaneKernel* k = find_plane_kernel(kprec(prec), c->ax[0].n);
+    if (!k) return GPUE_OK;
+    int max_smem = 0;
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+    if (k->smem > max_smem) return GPUE_OK;
+    int ncl = 1 << 30;
+    for (void (*fn)(PassArgs) : {k->fwd, k->inv}) {
+        CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, k->smem));
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(k->cs);
+        cfg.blockDim = dim3(k->threads);
+        cfg.dynamicSmemBytes = k->smem;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = k->cs;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int n = 0;
+        CK(cudaOccupancyMaxActiveClusters(&n, fn, &cfg));
+        ncl = std::min(ncl, n);
+    }
+    if (ncl < 1) return GPUE_OK;
+    ncl = std::min(ncl, c->ax[2].n);
+    pc.k = k;
+    pc.blocks = ncl * k->cs;
+    return GPUE_OK;
+}
+
+bool plane_ok(const gpue_ctx* c, int prec) {
+    if (!c->plane[prec].k || c->ext) return false;
+    return !(c->p.corotating && (axis_gauge_active(c, 0) || axis_gauge_active(c, 1)));
+}
+
 gpue_status make_pass_args(gpue_ctx* c, int prec, const LPass& lp, int gstate, PassArgs& a) {
-    const LaunchCfg& lc = c->lc[prec][lp.axis];
-    if (!lc.k) return fail(c, GPUE_ERR_STATE, "axis %d not planned", lp.axis);
-    if (lp.red != RED_NONE && lc.ntiles > c->partials_cap - kAuxPartials &&
-        lc.blocks > c->partials_cap - kAuxPartials)
-        return fail(c, GPUE_ERR_INVALID_ARG, "reduction grid %d exceeds scratch", lc.blocks);
+    const bool plane = lp.axis >= kPlaneFwd;
+    const int ax_i = plane ? 0 : lp.axis;  // the plane passes transform x (and y = x)
+    const LaunchCfg& lc = c->lc[prec][ax_i];
+    if (plane) {
+        if (!c->plane[prec].k) return fail(c, GPUE_ERR_STATE, "plane passes not planned");
+    } else {
+        if (!lc.k) return fail(c, GPUE_ERR_STATE, "axis %d not planned", lp.axis);
+        if (lp.red != RED_NONE && lc.ntiles > c->partials_cap - kAuxPartials &&
+            lc.blocks > c->partials_cap - kAuxPartials)
+            return fail(c, GPUE_ERR_INVALID_ARG, "reduction grid %d exceeds scratch", lc.blocks);
+    }
     const Tables& tb = c->tab[prec];
     const gpue_params& p = c->p;
     std::memset(&a, 0, sizeof a);
@@ -312,7 +379,7 @@ gpue_status make_pass_args(gpue_ctx* c, int prec, const LPass& lp, int gstate, P
     a.nx = c->ax[0].n;
     a.ny = c->ax[1].n;
     a.nz = c->ax[2].n;
-    a.ntiles = lc.ntiles;
+    a.ntiles = plane ? c->ax[2].n : lc.ntiles;
     a.nops = (int)lp.ops.size();
     for (int i = 0; i < a.nops; ++i) a.ops[i] = lp.ops[i];
     a.store = lp.store ? 1 : 0;
@@ -321,21 +388,23 @@ gpue_status make_pass_args(gpue_ctx* c, int prec, const LPass& lp, int gstate, P
     const double Dt = gstate == 0 ? p.gdt : p.dt;
     a.nl_coef = (p.interaction * p.gDenConst) * ((0.5 * Dt) / p.hbar);
     a.kscale = 1.0 / (double)c->N;
-    a.gscale = 1.0 / (double)c->ax[lp.axis].n;
+    a.gscale = 1.0 / (double)c->ax[ax_i].n;
     double axc, ayc;
     gauge_coefs(c, axc, ayc);
     a.gauge_coef = lp.axis == 0 ? axc : lp.axis == 1 ? ayc : 0.0;
     a.gauge_src = lp.axis == 0 ? 1 : 0;
     a.gauge_dt = lp.gauge_dt;
-    a.dmom = c->ax[lp.axis].n > 1 ? c->ax[lp.axis].p[1] : 0.0;
+    a.dmom = c->ax[ax_i].n > 1 ? c->ax[ax_i].p[1] : 0.0;
     a.kin_coef = p.hbar * p.hbar / (2 * p.mass);
     for (int i = 0; i < 3; ++i) {
         a.vfac[i] = tb.vfac[i];
         a.kfac[i] = tb.kfac[i];
+        a.vd[i] = tb.vd[i];
+        a.kd[i] = tb.kd[i];
         a.pos[i] = tb.pos[i];
         a.mom[i] = tb.mom[i];
     }
-    a.tw = tb.tw[lp.axis];
+    a.tw = tb.tw[ax_i];
     a.red.kind = lp.red;
     a.red.partials = c->partials;
     a.red.counter = c->counters + lp.ctr;
@@ -362,6 +431,7 @@ gpue_status make_pass_args(gpue_ctx* c, int prec, const LPass& lp, int gstate, P
         for (int i = 0; i < 3; ++i) prog(2 + i, a.prog_a[i], a.nprog_a[i]);
     }
     a.active = c->dflags;
+    a.err = c->dflags + 3;
     return GPUE_OK;
 }
 
@@ -371,6 +441,26 @@ gpue_status launch_pass(gpue_ctx* c, int prec, const LPass& lp, int gstate, bool
     gpue_status st = make_pass_args(c, prec, lp, gstate, a);
     if (st) return st;
     a.active = nullptr;  // a single solve always runs
+    if (lp.axis >= kPlaneFwd) {
+        const PlaneCfg& pc = c->plane[prec];
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(pc.blocks);
+        cfg.blockDim = dim3(pc.k->threads);
+        cfg.dynamicSmemBytes = pc.k->smem;
+        cfg.stream = c->stream;
+        cudaLaunchAttribute at[2];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = pc.k->cs;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[1].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = pdl ? 2 : 1;
+        CK(cudaLaunchKernelEx(&cfg, lp.axis == kPlaneFwd ? pc.k->fwd : pc.k->inv, a));
+        c->launches++;
+        return GPUE_OK;
+    }
     const LaunchCfg& lc = c->lc[prec][lp.axis];
     void (*fn)(PassArgs) = lp.axis == 0 ? (c->ext ? lc.k->row_ext : lc.k->row)
                                         : (c->ext ? lc.k->col_ext : lc.k->col);
@@ -383,7 +473,7 @@ gpue_status launch_pass(gpue_ctx* c, int prec, const LPass& lp, int gstate, bool
 // guard period (0 off): steps with i % guard == guard-1 end with a NORM, and
 // the factor is folded into the K pass of the next step (i % guard == 0).
 void step_passes(gpue_ctx* c, int i, int gstate, bool scale_first, double rexp, int guard,
-                 std::vector<LPass>& out) {
+                 std::vector<LPass>& out, bool plane) {
     const bool g_norm = guard > 0 && i % guard == guard - 1;
     const bool g_apply = guard > 0 && i % guard == 0;
     const bool imag = gstate == 0;
@@ -407,25 +497,36 @@ void step_passes(gpue_ctx* c, int i, int gstate, bool scale_first, double rexp, 
             if (ord[k] < c->dim && axis_gauge_active(c, ord[k])) gaxes.push_back(ord[k]);
     }
     std::vector<LPass> s;
-    std::vector<int> first;
-    if (scale_first) first.push_back(OP_SCALE);
-    first.push_back(OP_VHALF);
-    first.push_back(OP_FFT_F);
-    const int kaxis = c->dim == 3 ? 2 : 1;
-    s.push_back(P(0, first));
-    if (c->dim == 3) s.push_back(P(1, {OP_FFT_F}));
-    LPass kp = P(kaxis, {OP_FFT_F, OP_KPHASE, OP_FFT_I});
-    if (g_apply) kp.kscale_slot = kGuard;
-    s.push_back(kp);
-    if (c->dim == 3) s.push_back(P(1, {OP_FFT_I}));
-    size_t g0 = 0;
-    if (!gaxes.empty() && gaxes[0] == 0) {
-        s.push_back(P(0, {OP_FFT_I, OP_VHALF, OP_FFT_F, OP_GAUGE, OP_FFT_I}));
-        g0 = 1;
+    if (plane && c->dim == 3 && gaxes.empty()) {
+        // XY[scale V/2 Fx Fy] Z[Fz K Iz] XY[Ix Iy V/2]
+        LPass f = P(kPlaneFwd, {});
+        if (scale_first) f.ops.push_back(OP_SCALE);
+        s.push_back(f);
+        LPass kp = P(2, {OP_FFT_F, OP_KPHASE, OP_FFT_I});
+        if (g_apply) kp.kscale_slot = kGuard;
+        s.push_back(kp);
+        s.push_back(P(kPlaneInv, {}));
     } else {
-        s.push_back(P(0, {OP_FFT_I, OP_VHALF}));
+        std::vector<int> first;
+        if (scale_first) first.push_back(OP_SCALE);
+        first.push_back(OP_VHALF);
+        first.push_back(OP_FFT_F);
+        const int kaxis = c->dim == 3 ? 2 : 1;
+        s.push_back(P(0, first));
+        if (c->dim == 3) s.push_back(P(1, {OP_FFT_F}));
+        LPass kp = P(kaxis, {OP_FFT_F, OP_KPHASE, OP_FFT_I});
+        if (g_apply) kp.kscale_slot = kGuard;
+        s.push_back(kp);
+        if (c->dim == 3) s.push_back(P(1, {OP_FFT_I}));
+        size_t g0 = 0;
+        if (!gaxes.empty() && gaxes[0] == 0) {
+            s.push_back(P(0, {OP_FFT_I, OP_VHALF, OP_FFT_F, OP_GAUGE, OP_FFT_I}));
+            g0 = 1;
+        } else {
+            s.push_back(P(0, {OP_FFT_I, OP_VHALF}));
+        }
+        for (size_t k = g0; k < gaxes.size(); ++k) s.push_back(P(gaxes[k], {OP_FFT_F, OP_GAUGE, OP_FFT_I}));
     }
-    for (size_t k = g0; k < gaxes.size(); ++k) s.push_back(P(gaxes[k], {OP_FFT_F, OP_GAUGE, OP_FFT_I}));
     if (imag || g_norm) {
         LPass& last = s.back();
         last.ops.push_back(OP_NORM);
@@ -657,9 +758,10 @@ gpue_status enqueue_steps(gpue_ctx* c, int prec, int i0, int i1, int gstate, boo
     std::vector<LPass> v;
     // every imaginary-time step after the first renormalises the state the
     // previous step left (the deferred parSum scale)
+    const bool plane = plane_ok(c, prec);
     for (int i = i0; i < i1; ++i)
         step_passes(c, i, gstate, i == i0 ? scale_first : gstate == 0,
-                    rexp.empty() ? 1.0 : rexp[i], guard, v);
+                    rexp.empty() ? 1.0 : rexp[i], guard, v, plane);
     if (!c->time_dep) fuse(v);  // fused passes would mix two steps' times
     for (size_t k = 0; k < v.size(); ++k) {
         gpue_status st = launch_pass(c, prec, v[k], gstate, k > 0);
@@ -1033,6 +1135,8 @@ gpue_status gpue_ctx_create(const gpue_params* p, gpue_ctx** out) {
         st = plan_axis(c, c->prec, a);
         if (st) return st;
     }
+    st = plan_plane(c, c->prec);
+    if (st) return st;
     const char* tune = std::getenv("GPUE_AUTOTUNE");
     if (tune && tune[0] == '1') {
         st = autotune_ctx(c, c->prec, false);
@@ -1577,6 +1681,14 @@ gpue_status gpue_evolve(gpue_ctx* c, int32_t nsteps, int32_t gstate,
     CK(cudaEventSynchronize(c->ev1));
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    if (c->plane[c->prec].k) {
+        int gave_up = 0;
+        CK(cudaMemcpy(&gave_up, c->dflags + 3, sizeof gave_up, cudaMemcpyDeviceToHost));
+        if (gave_up) {
+            CK(cudaMemset(c->dflags + 3, 0, sizeof gave_up));
+            return fail(c, GPUE_ERR_TIMEOUT, "a plane pass gave up waiting for its data");
+        }
+    }
     if (res) {
         std::memset(res, 0, sizeof *res);
         res->steps_done = lo.done;

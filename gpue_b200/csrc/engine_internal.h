@@ -44,6 +44,8 @@ struct Tables {
     const double* pos[3] = {};
     const double* mom[3] = {};
     const double* vreal[3] = {};
+    const float2* vd[3] = {};   // complex64 forms: V/2 and K factors minus 1, as float2
+    const float2* kd[3] = {};
     int built_for = -1;  // gstate of vfac/kfac
 };
 
@@ -56,6 +58,15 @@ struct LaunchCfg {
     bool tuned = false;     // chosen by the autotuner
     float us = 0, default_us = 0;  // tuned and default pass times (FFT round trip)
 };
+
+// XY-plane passes of a 3D context (plane.cuh): the kernel pair and the
+// persistent grid (whole clusters)
+struct PlaneCfg {
+    const PlaneKernel* k = nullptr;
+    int blocks = 0;
+};
+// LPass::axis values of the two plane passes
+enum { kPlaneFwd = 3, kPlaneInv = 4 };
 
 struct GraphKey {
     int prec, gstate, parity, nsteps, scale_first, energy_last, guard, observables;
@@ -90,9 +101,11 @@ struct gpue_ctx {
     double2* partials = nullptr;
     long partials_cap = 0;
     unsigned* counters = nullptr;
-    int* dflags = nullptr;       // [0] active (batched runs), [1] steps when converged
+    int* dflags = nullptr;       // [0] active (batched runs), [1] steps when converged,
+                                 // [3] a bounded device wait gave up
     gpue_eng::Tables tab[2];            // indexed by GPUE_PREC_*
     gpue_eng::LaunchCfg lc[2][3];       // [precision][axis]
+    gpue_eng::PlaneCfg plane[2];        // [precision]: XY-plane passes, if any
     bool have_wfc = false;
     bool pending_scale = false;  // scal[kScale] must multiply psi
     std::map<gpue_eng::GraphKey, gpue_eng::Segment> graphs;
@@ -198,8 +211,15 @@ gpue_status plan_axis(gpue_ctx* c, int prec, int axis);
 // and keeps the fastest for each axis (cached per shape for the process).
 gpue_status autotune_ctx(gpue_ctx* c, int prec, bool force);
 gpue_status make_pass_args(gpue_ctx* c, int prec, const LPass& lp, int gstate, PassArgs& a);
+// plane: run the in-plane axes of a 3D step as the two XY-plane passes
 void step_passes(gpue_ctx* c, int i, int gstate, bool scale_first, double rexp, int guard,
-                 std::vector<LPass>& out);
+                 std::vector<LPass>& out, bool plane = false);
+// Plans the XY-plane passes of precision prec when the context qualifies
+// (3D, nx = ny with a compiled plane kernel); leaves them off otherwise.
+gpue_status plan_plane(gpue_ctx* c, int prec);
+// The plane passes can run this context's steps now (no table or expression
+// fields, no in-plane gauge).
+bool plane_ok(const gpue_ctx* c, int prec);
 void fuse(std::vector<LPass>& v);
 std::vector<LPass> energy_passes(const gpue_ctx* c, bool scale_pending);
 EnergyArgs energy_args(gpue_ctx* c, int prec, bool scale_pending);

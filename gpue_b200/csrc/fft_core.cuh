@@ -254,7 +254,20 @@ struct LineFFT {
     // multiple of Ns they depend on t only and one set serves every group.
     // Larger sets (long odd-radix plans) are read at use, as registers are
     // scarce there.
-    template <int S>
+    // TWS: the twiddle table is in shared memory (plain loads), else global
+    // (read-only cache)
+    template <bool TWS>
+    static __device__ __forceinline__ float4 tw4(const float4* p) {
+        if constexpr (TWS) return *p;
+        else return __ldg(p);
+    }
+    template <bool TWS>
+    static __device__ __forceinline__ cx<T> tw1(const cx<T>* p) {
+        if constexpr (TWS) return *p;
+        else return *p;
+    }
+
+    template <int S, bool TWS = false>
     struct StageTw {
         static constexpr int R = radix(S);
         static constexpr int Ns = ns_before(S);
@@ -281,11 +294,11 @@ struct LineFFT {
                     for (int r = 1; r < R; ++r) {
                         const int k = jm * r * step;
                         if constexpr (SPLIT) {
-                            const float4 e = __ldg(reinterpret_cast<const float4*>(tw) + k);
+                            const float4 e = tw4<TWS>(reinterpret_cast<const float4*>(tw) + k);
                             w[q][r - 1][0] = cx<T>{e.x, e.y};
                             w[q][r - 1][WPER - 1] = cx<T>{e.z, e.w};
                         } else {
-                            w[q][r - 1][0] = tw[k];
+                            w[q][r - 1][0] = tw1<TWS>(tw + k);
                         }
                     }
                 }
@@ -299,17 +312,17 @@ struct LineFFT {
             } else {
                 const int k = ((t + P * q) % Ns) * r * step;
                 if constexpr (SPLIT) {
-                    const float4 e = __ldg(reinterpret_cast<const float4*>(tw) + k);
+                    const float4 e = tw4<TWS>(reinterpret_cast<const float4*>(tw) + k);
                     return cmul_split(a, cx<float>{e.x, e.y}, cx<float>{e.z, e.w});
                 } else {
-                    return cmul(a, tw[k]);
+                    return cmul(a, tw1<TWS>(tw + k));
                 }
             }
         }
     };
 
-    template <int S>
-    static __device__ __forceinline__ void compute(cx<T> (&v)[E], const StageTw<S>* w) {
+    template <int S, bool TWS = false>
+    static __device__ __forceinline__ void compute(cx<T> (&v)[E], const StageTw<S, TWS>* w) {
         constexpr int R = radix(S);
         constexpr int G = N / (R * P);
 #pragma unroll
@@ -349,23 +362,24 @@ struct LineFFT {
 
     // One stage after the first: its twiddles are requested before the
     // exchange, so their latency overlaps the shared-memory round trip.
-    template <int S, typename Sync>
+    template <int S, bool TWS, typename Sync>
     static __device__ __forceinline__ void stage(cx<T> (&v)[E], int t, cx<T>* sl,
                                                  const cx<T>* __restrict__ tw, Sync sync) {
-        StageTw<S> w;
+        StageTw<S, TWS> w;
         w.load(t, tw);
         exchange<S - 1>(v, t, sl, sync);
-        compute<S>(v, &w);
+        compute<S, TWS>(v, &w);
     }
 
     // Unnormalised forward DFT of the line (inverse: conjugate around it).
-    template <typename Sync>
+    // TWS: tw points to a copy of the table in shared memory.
+    template <bool TWS = false, typename Sync>
     static __device__ __forceinline__ void forward(cx<T> (&v)[E], int t, cx<T>* sl,
                                                    const cx<T>* __restrict__ tw, Sync sync) {
-        compute<0>(v, static_cast<const StageTw<0>*>(nullptr));
-        stage<1>(v, t, sl, tw, sync);
-        if constexpr (NS >= 3) stage<2>(v, t, sl, tw, sync);
-        if constexpr (NS >= 4) stage<3>(v, t, sl, tw, sync);
+        compute<0, TWS>(v, static_cast<const StageTw<0, TWS>*>(nullptr));
+        stage<1, TWS>(v, t, sl, tw, sync);
+        if constexpr (NS >= 3) stage<2, TWS>(v, t, sl, tw, sync);
+        if constexpr (NS >= 4) stage<3, TWS>(v, t, sl, tw, sync);
     }
 };
 

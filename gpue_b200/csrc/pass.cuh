@@ -86,6 +86,8 @@ struct PassArgs {
     double kin_coef;    // hbar^2 / (2 m), for OP_EKIN
     const double2* vfac[3];  // per-axis V half-step factor (FP64)
     const double2* kfac[3];  // per-axis kinetic factor (FP64)
+    const float2* vd[3];     // complex64 form: the V/2 factor minus 1, rounded once
+    const float2* kd[3];     // complex64 form: the kinetic factor minus 1
     const double* pos[3];
     const double* mom[3];
     const void* tw;  // W_N^k for this axis: cx<double>[N], or (hi, lo) float pairs [N]
@@ -107,6 +109,7 @@ struct PassArgs {
     double grid_d[3];        // dx, dy, dz as evolve() passes them (1 for absent axes)
     double hbar;
     const int* active;       // batched solves: 0 once converged (skip the tiles)
+    int* err;                // plane passes: set non-zero when a bounded wait gave up
 };
 
 // ------------------------------------------------------- FP64 reductions --
@@ -276,6 +279,193 @@ __device__ __forceinline__ double decay(double a) {
     else return (double)expf((float)-a);
 }
 
+// OP_VHALF with separable factors: psi *= fa[k] * lf * (nonlinear factor),
+// fa the pass axis' FP64 V/2 factors, lf the product of the other axes' at the
+// line.  The nonlinear angle gN|psi|^2 Dt/(2 hbar) is almost always below 1/16,
+// where a Taylor series is exact to FP64: that is decided once for the
+// thread's values (an FP32 estimate with margin), so the unrolled loops have
+// no branch and the values' FP64 chains interleave.
+template <typename T, class L>
+__device__ __forceinline__ void op_vhalf_sep(cx<T> (&v)[L::E], int t, const double2* fa,
+                                             cx<double> lf, const PassArgs& a) {
+    constexpr int E = L::E;
+    bool small = true;
+    if (a.gpe) {
+        const float nl = (float)a.nl_coef;
+        float m = 0.f;
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+            m = fmaxf(m, fabsf(nl * ((float)v[e].x * (float)v[e].x +
+                                     (float)v[e].y * (float)v[e].y)));
+        small = m < 0.06f;
+    }
+    if (!a.gpe) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) v[e] = apply(v[e], cmul(ld2(fa, L::index(t, e)), lf));
+    } else if (small && a.gstate == 0) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const double gd = a.nl_coef * ((double)v[e].x * v[e].x + (double)v[e].y * v[e].y);
+            const cx<double> f = cmul(ld2(fa, L::index(t, e)), lf);
+            v[e] = apply(v[e], cscale(f, taylor_decay(gd)));
+        }
+    } else if (small) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const double gd = a.nl_coef * ((double)v[e].x * v[e].x + (double)v[e].y * v[e].y);
+            const cx<double> f = cmul(ld2(fa, L::index(t, e)), lf);
+            v[e] = apply(v[e], cmul(f, taylor_phase(gd)));
+        }
+    } else {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            cx<double> f = cmul(ld2(fa, L::index(t, e)), lf);
+            const double gd = a.nl_coef * ((double)v[e].x * v[e].x + (double)v[e].y * v[e].y);
+            if (a.gstate == 0) f = cscale(f, small_decay<T>(gd));
+            else f = cmul(f, small_phase<T>(gd));
+            v[e] = apply(v[e], f);
+        }
+    }
+}
+
+// OP_NORM: the thread's E terms summed in plain FP64 (relative error
+// ~E * 2^-53), entering the compensated sum once per line.
+template <typename T, int E>
+__device__ __forceinline__ void op_norm(const cx<T> (&v)[E], KSum& acc) {
+    double part = 0.0;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const double re = (double)v[e].x, im = (double)v[e].y;
+        part += re * re + im * im;
+    }
+    acc.add(part);
+}
+
+// ------------------------------------------------ complex64 phase factors --
+//
+// The complex64 form carries each factor f as d = f - 1, formed in FP64 (or
+// higher) and rounded once to FP32, and applies it as psi + d*psi: the small
+// correction d*psi is formed in FP32 and added with one rounding of psi's
+// magnitude, which is as accurate as an FP64 product rounded once and keeps
+// |f| = 1 of a real-time factor to FP32 round-off relative to |d|, with no
+// systematic growth.  Products of separable factors combine as
+// (1 + a)(1 + b) - 1 = a + b + a*b (no cancellation: the angles of one
+// factor kind share a sign).
+
+__device__ __forceinline__ float2 dmul(float2 a, float2 b) {
+    float rx = a.x + b.x, ry = a.y + b.y;
+    rx = fmaf(a.x, b.x, fmaf(-a.y, b.y, rx));
+    ry = fmaf(a.x, b.y, fmaf(a.y, b.x, ry));
+    return {rx, ry};
+}
+// psi + d*psi
+__device__ __forceinline__ cx<float> dapply(cx<float> v, float2 d) {
+    const float cx_ = fmaf(d.x, v.x, -d.y * v.y);
+    const float cy_ = fmaf(d.x, v.y, d.y * v.x);
+    return {v.x + cx_, v.y + cy_};
+}
+// psi + d*psi for a real d
+__device__ __forceinline__ cx<float> dapply_re(cx<float> v, float d) {
+    return {fmaf(d, v.x, v.x), fmaf(d, v.y, v.y)};
+}
+// f - 1 of an FP64 factor f near 1, rounded to FP32
+__device__ __forceinline__ float2 line_delta(cx<double> f) {
+    return {(float)(f.x - 1.0), (float)f.y};
+}
+__device__ __forceinline__ float2 ldf2(const float2* p, int i) { return p[i]; }
+
+// exp(-i p) - 1 and exp(-p) - 1 for |p| < 1/16 by their Taylor series in
+// FP32 (truncation below 2^-24 relative)
+__device__ __forceinline__ float2 nl_phase_delta(float p) {
+    const float p2 = p * p;
+    const float sn = p * fmaf(-p2 * (1.f / 6.f), fmaf(-p2, 1.f / 20.f, 1.f), 1.f);
+    const float cm = -0.5f * p2 * fmaf(-p2 * (1.f / 12.f), fmaf(-p2, 1.f / 30.f, 1.f), 1.f);
+    return {cm, -sn};
+}
+__device__ __forceinline__ float nl_decay_delta(float p) {
+    float r = fmaf(-p, 1.f / 120.f, 1.f / 24.f);
+    r = fmaf(-p, r, 1.f / 6.f);
+    r = fmaf(-p, r, 0.5f);
+    r = fmaf(-p, r, 1.f);
+    return -p * r;
+}
+// the same for any p, in FP64 from the FP64 angle, rounded once
+__device__ __forceinline__ float2 nl_phase_delta64(double p) {
+    double s, c;
+    sincos(p, &s, &c);
+    const double h = sin(0.5 * p);
+    return {(float)(-2.0 * h * h), (float)(-s)};
+}
+__device__ __forceinline__ float nl_decay_delta64(double p) { return (float)expm1(-p); }
+
+// OP_VHALF, complex64, separable V: psi *= (1 + dl)(1 + dk[k]) * nonlinear
+// factor, dl the other axes' factors at the line (minus 1).  nl64 is the
+// nonlinear coefficient for the density of the values in v (a.nl_coef, times
+// s^2 when a pending scale s is folded into dl instead of applied to v).
+template <class L>
+__device__ __forceinline__ void op_vhalf_f32(cx<float> (&v)[L::E], int t, const float2* dk,
+                                             float2 dl, const PassArgs& a, double nl64) {
+    constexpr int E = L::E;
+    const float nl = (float)nl64;
+    bool small = true;
+    if (a.gpe) {
+        float m = 0.f;
+#pragma unroll
+        for (int e = 0; e < E; ++e) m = fmaxf(m, fabsf(nl * fmaf(v[e].x, v[e].x, v[e].y * v[e].y)));
+        small = m < 0.06f;
+    }
+    if (!a.gpe) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) v[e] = dapply(v[e], dmul(dl, ldf2(dk, L::index(t, e))));
+    } else if (small && a.gstate == 0) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const float dv = dl.x + ldf2(dk, L::index(t, e)).x +
+                             dl.x * ldf2(dk, L::index(t, e)).x;
+            const float dn = nl_decay_delta(nl * fmaf(v[e].x, v[e].x, v[e].y * v[e].y));
+            v[e] = dapply_re(v[e], fmaf(dv, dn, dv + dn));
+        }
+    } else if (small) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const float2 dn = nl_phase_delta(nl * fmaf(v[e].x, v[e].x, v[e].y * v[e].y));
+            v[e] = dapply(v[e], dmul(dmul(dl, ldf2(dk, L::index(t, e))), dn));
+        }
+    } else {
+        // large nonlinear angles: the factor from the FP64 angle in FP64
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const double p = nl64 * ((double)v[e].x * v[e].x + (double)v[e].y * v[e].y);
+            const float2 dv = dmul(dl, ldf2(dk, L::index(t, e)));
+            const float2 dn = a.gstate == 0 ? float2{nl_decay_delta64(p), 0.f}
+                                            : nl_phase_delta64(p);
+            v[e] = dapply(v[e], dmul(dv, dn));
+        }
+    }
+}
+
+// OP_KPHASE, complex64, separable K: psi *= s (1 + dl)(1 + dk[k]), s the
+// real scalings (1/N, the norm guard)
+template <class L>
+__device__ __forceinline__ void op_kphase_f32(cx<float> (&v)[L::E], int t, const float2* dk,
+                                              float2 dl, float s) {
+#pragma unroll
+    for (int e = 0; e < L::E; ++e) {
+        const cx<float> w = dapply(v[e], dmul(dl, ldf2(dk, L::index(t, e))));
+        v[e] = {w.x * s, w.y * s};
+    }
+}
+
+// OP_NORM, complex64: the thread's |psi|^2 summed in FP32 (relative error
+// ~E 2^-24 per thread, unbiased), entering the FP64 compensated sum once
+template <int E>
+__device__ __forceinline__ void op_norm_f32(const cx<float> (&v)[E], KSum& acc) {
+    float part = 0.f;
+#pragma unroll
+    for (int e = 0; e < E; ++e) part += fmaf(v[e].x, v[e].x, v[e].y * v[e].y);
+    acc.add((double)part);
+}
+
 // ---------------------------------------------------------------- kernel --
 
 constexpr int kMaxPassThreads = 256;
@@ -421,53 +611,10 @@ __device__ __forceinline__ KSum pass_tiles(const PassArgs& a, long t0, long tste
                     if (a.axis == 0) lf = cmul(ld2(a.vfac[1], yi), ld2(a.vfac[2], zi));
                     else if (a.axis == 1) lf = cmul(ld2(a.vfac[0], xi), ld2(a.vfac[2], zi));
                     else lf = cmul(ld2(a.vfac[0], xi), ld2(a.vfac[1], yi));
-                    const double2* fa = a.vfac[a.axis];
-                    // The nonlinear angle gN|psi|^2 Dt/(2 hbar) is almost always
-                    // below 1/16, where a Taylor series is exact to FP64: decide
-                    // that once for the thread's values (an FP32 estimate with
-                    // margin), so the unrolled loop below has no branch and the
-                    // values' FP64 chains interleave.
-                    bool small = true;
-                    if (a.gpe) {
-                        const float nl = (float)a.nl_coef;
-                        float m = 0.f;
-#pragma unroll
-                        for (int e = 0; e < E; ++e)
-                            m = fmaxf(m, fabsf(nl * ((float)v[e].x * (float)v[e].x +
-                                                     (float)v[e].y * (float)v[e].y)));
-                        small = m < 0.06f;
-                    }
-                    if (!a.gpe) {
-#pragma unroll
-                        for (int e = 0; e < E; ++e)
-                            v[e] = apply(v[e], cmul(ld2(fa, L::index(t, e)), lf));
-                    } else if (small && a.gstate == 0) {
-#pragma unroll
-                        for (int e = 0; e < E; ++e) {
-                            const double gd = a.nl_coef * ((double)v[e].x * v[e].x +
-                                                           (double)v[e].y * v[e].y);
-                            const cx<double> f = cmul(ld2(fa, L::index(t, e)), lf);
-                            v[e] = apply(v[e], cscale(f, taylor_decay(gd)));
-                        }
-                    } else if (small) {
-#pragma unroll
-                        for (int e = 0; e < E; ++e) {
-                            const double gd = a.nl_coef * ((double)v[e].x * v[e].x +
-                                                           (double)v[e].y * v[e].y);
-                            const cx<double> f = cmul(ld2(fa, L::index(t, e)), lf);
-                            v[e] = apply(v[e], cmul(f, taylor_phase(gd)));
-                        }
-                    } else {
-#pragma unroll
-                        for (int e = 0; e < E; ++e) {
-                            cx<double> f = cmul(ld2(fa, L::index(t, e)), lf);
-                            const double gd = a.nl_coef * ((double)v[e].x * v[e].x +
-                                                           (double)v[e].y * v[e].y);
-                            if (a.gstate == 0) f = cscale(f, small_decay<T>(gd));
-                            else f = cmul(f, small_phase<T>(gd));
-                            v[e] = apply(v[e], f);
-                        }
-                    }
+                    if constexpr (std::is_same<T, float>::value)
+                        op_vhalf_f32<L>(v, t, a.vd[a.axis], line_delta(lf), a, a.nl_coef);
+                    else
+                        op_vhalf_sep<T, L>(v, t, a.vfac[a.axis], lf, a);
                     break;
                 }
                 case OP_KPHASE: {
@@ -495,10 +642,16 @@ __device__ __forceinline__ KSum pass_tiles(const PassArgs& a, long t0, long tste
                     if (a.axis == 0) lf = cmul(ld2(a.kfac[1], yi), ld2(a.kfac[2], zi));
                     else if (a.axis == 1) lf = cmul(ld2(a.kfac[0], xi), ld2(a.kfac[2], zi));
                     else lf = cmul(ld2(a.kfac[0], xi), ld2(a.kfac[1], yi));
-                    lf = cscale(lf, a.kscale_in ? a.kscale * *a.kscale_in : a.kscale);
-                    const double2* fa = a.kfac[a.axis];
+                    const double ks = a.kscale_in ? a.kscale * *a.kscale_in : a.kscale;
+                    if constexpr (std::is_same<T, float>::value) {
+                        op_kphase_f32<L>(v, t, a.kd[a.axis], line_delta(lf), (float)ks);
+                    } else {
+                        lf = cscale(lf, ks);
+                        const double2* fa = a.kfac[a.axis];
 #pragma unroll
-                    for (int e = 0; e < E; ++e) v[e] = apply(v[e], cmul(ld2(fa, L::index(t, e)), lf));
+                        for (int e = 0; e < E; ++e)
+                            v[e] = apply(v[e], cmul(ld2(fa, L::index(t, e)), lf));
+                    }
                     break;
                 }
                 case OP_GAUGE: {
@@ -577,18 +730,10 @@ __device__ __forceinline__ KSum pass_tiles(const PassArgs& a, long t0, long tste
                     }
                     break;
                 }
-                // The thread's E terms are summed in plain FP64 (relative
-                // error ~E * 2^-53) and enter the compensated sum once per tile.
-                case OP_NORM: {
-                    double part = 0.0;
-#pragma unroll
-                    for (int e = 0; e < E; ++e) {
-                        const double re = (double)v[e].x, im = (double)v[e].y;
-                        part += re * re + im * im;
-                    }
-                    acc.add(part);
+                case OP_NORM:
+                    if constexpr (std::is_same<T, float>::value) op_norm_f32<E>(v, acc);
+                    else op_norm<T, E>(v, acc);
                     break;
-                }
                 case OP_EKIN: {
                     double part = 0.0;
 #pragma unroll

@@ -23,6 +23,21 @@ struct PassKernel {
     void (*col_batch)(const PassArgs*, const long*, int);
 };
 
+// An XY-plane pass pair for 3D fields with nx = ny = n (plane.cuh): a cluster
+// of cs CTAs of `threads` threads and `smem` bytes of dynamic shared memory
+// per plane, persistent over the z-planes.
+struct PlaneKernel {
+    int n;
+    int ra, rb, rc, p;  // the line FFT plan of both in-plane transforms
+    int cs;             // CTAs per cluster
+    int threads;
+    int smem;
+    void (*fwd)(PassArgs);  // rows [scale] V/2 Fx, columns Fy
+    void (*inv)(PassArgs);  // rows Ix, columns Iy V/2 [norm]
+};
+// nullptr when no plane pass is compiled for (precision, n)
+const PlaneKernel* find_plane_kernel(int prec, int n);
+
 // The default plan for a length; nullptr when none is compiled
 const PassKernel* find_pass_kernel(int prec, int n);
 // All plans for a length, default first; returns how many (at most cap)

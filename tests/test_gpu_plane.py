@@ -1,0 +1,73 @@
+"""The XY-plane passes (plane.cuh) of the complex64 3D step against the
+oracle and against the five-pass line schedule.
+
+A 3D FP32 context with nx = ny of a length that has a plane kernel runs its
+steps as XY[scale V/2 Fx Fy] Z[Fz K Iz] XY[Ix Iy V/2 norm]; GPUE_PLANE=0 at
+context creation keeps the line passes.  Both schedules are the same
+arithmetic in another order, so they agree to complex64 round-off; both are
+checked against the FP64 oracle with the FP32 tolerances of the other parity
+tests (wavefunction L2 <= 1e-5, relative energy <= 1e-5).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import cases
+from helpers import dV, oracle_problem, product_params
+
+pytestmark = pytest.mark.gpu
+
+PLANE_LENGTHS = [64, 96, 128, 160, 192, 256]
+
+
+def run(c, steps, gstate, plane, psi0):
+    import gpue_b200 as G
+    old = os.environ.get("GPUE_PLANE")
+    os.environ["GPUE_PLANE"] = "1" if plane else "0"
+    try:
+        with G.Solver(product_params(c, G.PREC_FP32)) as s:
+            s.set_wfc(psi0)
+            r = s.evolve(steps, gstate, energy_every=c["energy_every"])
+            return s.get_wfc(), s.energy(), r
+    finally:
+        if old is None:
+            del os.environ["GPUE_PLANE"]
+        else:
+            os.environ["GPUE_PLANE"] = old
+
+
+@pytest.mark.parametrize("gstate", [0, 1], ids=["imag", "real"])
+@pytest.mark.parametrize("n", PLANE_LENGTHS)
+def test_plane_schedule_matches_oracle_and_line_schedule(n, gstate):
+    steps = 12 if n <= 128 else 4
+    c = dict(cases.DEFAULTS, dim=3, n=n, box=8.0, wz=2.5, g=200.0, gdt=1e-4, dt=1e-4,
+             seed=500 + n, init="gauss" if gstate == 0 else "phase",
+             energy_every=steps // 2)
+    psi0 = cases.initial_psi(c)
+    got, E, r = run(c, steps, gstate, True, psi0)
+    lines, El, rl = run(c, steps, gstate, False, psi0)
+    P = oracle_problem(c)
+    ref, res, en = P.evolve(psi0, steps, gstate)
+    Eref = P.energy(ref)
+    for psi, e in ((got, E), (lines, El)):
+        assert float(np.sqrt(np.sum(np.abs(psi - ref) ** 2) * dV(c))) <= 1e-5
+        assert abs(e - Eref) <= 1e-5 * abs(Eref)
+    assert float(np.sqrt(np.sum(np.abs(got - lines) ** 2) * dV(c))) <= 1e-5
+    assert r["n_energies"] == rl["n_energies"] == res["n_energies"]
+    assert abs(r["energy"] - en[-1]) <= 1e-5 * abs(en[-1])
+    # three passes per step instead of five
+    assert r["kernel_launches"] < rl["kernel_launches"]
+
+
+def test_plane_passes_chosen_only_where_they_apply():
+    """Gauge fields in the plane keep the line passes (same results as the
+    oracle either way); FP64 contexts have no plane kernels."""
+    import gpue_b200 as G
+    c = dict(cases.DEFAULTS, dim=3, n=64, box=8.0, wz=2.0, g=100.0, omega=0.4, gauge=True,
+             dt=1e-4, seed=77, init="phase", energy_every=0)
+    psi0 = cases.initial_psi(c)
+    got, E, r = run(c, 6, 1, True, psi0)
+    lines, El, rl = run(c, 6, 1, False, psi0)
+    assert r["kernel_launches"] == rl["kernel_launches"]
+    assert np.array_equal(got, lines)
