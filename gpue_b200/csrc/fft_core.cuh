@@ -267,6 +267,33 @@ struct LineFFT {
         else return *p;
     }
 
+    // TWS tables are laid out per stage: stage S's twiddles W_{Ns R}^{jm r}
+    // (jm = j mod Ns, 0 < r < R) at stage_base(S) + (r - 1) Ns + jm, so the
+    // threads of a warp (consecutive jm) read consecutive entries.
+    __host__ __device__ static constexpr int stage_base(int S) {
+        int b = 0;
+        for (int s = 1; s < S; ++s) b += (radix(s) - 1) * ns_before(s);
+        return b;
+    }
+    static constexpr int kStageTableLen = stage_base(NS);
+    // Fills the per-stage table (float4 (hi, lo) pairs or cx<T>) from the
+    // per-N table W_N^k; threads tid of nthreads share the work.
+    template <typename W>
+    static __device__ __forceinline__ void build_stage_table(W* dst, const W* __restrict__ src,
+                                                             int tid, int nthreads) {
+        for (int i = tid; i < kStageTableLen; i += nthreads) {
+            int S = 1;
+            while (S + 1 < NS && i >= stage_base(S + 1)) ++S;
+            const int Ns = ns_before(S), R = radix(S), off = i - stage_base(S);
+            const int r = off / Ns + 1, jm = off % Ns;
+            dst[i] = src[jm * r * (N / (Ns * R))];
+        }
+    }
+    template <int S>
+    static __device__ __forceinline__ int tw_index(int jm, int r) {
+        return stage_base(S) + (r - 1) * ns_before(S) + jm;
+    }
+
     template <int S, bool TWS = false>
     struct StageTw {
         static constexpr int R = radix(S);
@@ -292,7 +319,7 @@ struct LineFFT {
                     const int jm = (t + P * q) % Ns;
 #pragma unroll
                     for (int r = 1; r < R; ++r) {
-                        const int k = jm * r * step;
+                        const int k = TWS ? tw_index<S>(jm, r) : jm * r * step;
                         if constexpr (SPLIT) {
                             const float4 e = tw4<TWS>(reinterpret_cast<const float4*>(tw) + k);
                             w[q][r - 1][0] = cx<T>{e.x, e.y};
@@ -310,7 +337,8 @@ struct LineFFT {
                 if constexpr (SPLIT) return cmul_split(a, w[qq][r - 1][0], w[qq][r - 1][1]);
                 else return cmul(a, w[qq][r - 1][0]);
             } else {
-                const int k = ((t + P * q) % Ns) * r * step;
+                const int k = TWS ? tw_index<S>((t + P * q) % Ns, r)
+                                  : ((t + P * q) % Ns) * r * step;
                 if constexpr (SPLIT) {
                     const float4 e = tw4<TWS>(reinterpret_cast<const float4*>(tw) + k);
                     return cmul_split(a, cx<float>{e.x, e.y}, cx<float>{e.z, e.w});
@@ -372,7 +400,8 @@ struct LineFFT {
     }
 
     // Unnormalised forward DFT of the line (inverse: conjugate around it).
-    // TWS: tw points to a copy of the table in shared memory.
+    // TWS: tw points to the per-stage table (build_stage_table) in shared
+    // memory.
     template <bool TWS = false, typename Sync>
     static __device__ __forceinline__ void forward(cx<T> (&v)[E], int t, cx<T>* sl,
                                                    const cx<T>* __restrict__ tw, Sync sync) {

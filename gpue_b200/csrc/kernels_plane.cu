@@ -7,10 +7,11 @@
 namespace gpue {
 
 #define GPUE_PLANE(T, N, RA, RB, RC, P)                                                     \
-    PlaneKernel{N, RA, RB, RC, P, PlaneShape<T, N, RA, RB, P, RC>::CS,                       \
-                PlaneShape<T, N, RA, RB, P, RC>::THREADS,                                    \
-                (int)PlaneShape<T, N, RA, RB, P, RC>::SMEM,                                  \
-                &k_plane<T, N, RA, RB, P, RC, false>, &k_plane<T, N, RA, RB, P, RC, true>}
+    PlaneKernel{N, RA, RB, RC, P, PlaneShape<T, N, RA, RB, P, RC, 16>::CS,                   \
+                PlaneShape<T, N, RA, RB, P, RC, 16>::THREADS,                                \
+                (int)PlaneShape<T, N, RA, RB, P, RC, 16>::SMEM,                              \
+                &k_plane<T, N, RA, RB, P, RC, 16, false>,                                    \
+                &k_plane<T, N, RA, RB, P, RC, 16, true>}
 
 static const PlaneKernel kPlanesF32[] = {
     GPUE_PLANE(float, 64, 4, 4, 0, 16),

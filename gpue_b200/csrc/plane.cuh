@@ -124,12 +124,16 @@ constexpr unsigned kPlaneWaitPolls = 1u << 22;
 
 // ------------------------------------------------------------ the kernel --
 
-template <typename T, int N, int RA, int RB, int P, int RC>
+// LPR_ = 16: two rounds of 16 lines per phase, 16 P threads, two CTAs per SM
+// (measured faster on the 256^3 ground state than one 32-line round of 32 P
+// threads at one CTA per SM: 145 vs 185 us per pass)
+template <typename T, int N, int RA, int RB, int P, int RC, int LPR_ = 16>
 struct PlaneShape {
     using L = LineFFT<T, N, RA, RB, P, RC>;
     static constexpr int E = L::E;
     static constexpr int RPC = 32;         // rows (then columns) per CTA
-    static constexpr int LPR = 16;         // lines transformed at once (a round)
+    static constexpr int LPR = LPR_;       // lines transformed at once (a round)
+    static constexpr int MINB = 512 / (LPR_ * P) > 1 ? 512 / (LPR_ * P) : 1;  // CTAs per SM
     static constexpr int CS = N / RPC;     // CTAs per cluster: one plane
     static constexpr int THREADS = LPR * P;
     static constexpr int LSR = L::LS;      // row stride of X (elements)
@@ -139,10 +143,11 @@ struct PlaneShape {
     static constexpr size_t SB = (size_t)LPR * SLS * sizeof(cx<T>);
     static constexpr size_t TWB = (size_t)N * 16;       // (hi, lo) float pairs
     static constexpr size_t DB = (size_t)N * sizeof(float2);  // one axis' factor - 1
-    static constexpr size_t SMEM = XB + SB + TWB + 2 * DB + 16;  // + the mbarrier
+    static constexpr size_t SMEM = XB + SB + TWB + 2 * DB + 16;  // + two mbarriers
     static_assert(std::is_same<T, float>::value, "complex64 plane passes");
     static_assert(N % RPC == 0 && CS >= 1 && CS <= 8, "plane of 32-row slices, <= 8 CTAs");
     static_assert(P <= 32 && 32 % P == 0, "a row's threads sit in one warp");
+    static_assert(RPC % LPR == 0 && (LPR == 16 || LPR == 32), "whole rounds of lines");
     static_assert((LSR * sizeof(cx<T>)) % 16 == 0 && (N * sizeof(cx<T>)) % 16 == 0,
                   "row slots and rows are whole 16-byte units (bulk copies)");
     static_assert(XB % 16 == 0 && SB % 16 == 0, "16-byte regions");
@@ -152,14 +157,16 @@ struct PlaneShape {
 // INV = true:  rows Ix, columns Iy V/2 [norm].
 // a.ops[0] != 0 asks for the deferred scale (forward pass only); a.red.kind
 // RED_NORM for the norm (inverse pass only).
-template <typename T, int N, int RA, int RB, int P, int RC, bool INV>
-__global__ void __launch_bounds__(PlaneShape<T, N, RA, RB, P, RC>::THREADS, 2)
+template <typename T, int N, int RA, int RB, int P, int RC, int LPR_, bool INV>
+__global__ void __launch_bounds__(PlaneShape<T, N, RA, RB, P, RC, LPR_>::THREADS,
+                                  PlaneShape<T, N, RA, RB, P, RC, LPR_>::MINB)
     k_plane(const PassArgs a) {
-    using S_ = PlaneShape<T, N, RA, RB, P, RC>;
+    using S_ = PlaneShape<T, N, RA, RB, P, RC, LPR_>;
     using L = typename S_::L;
     constexpr int E = S_::E;
     constexpr int RPC = S_::RPC;
     constexpr int LPR = S_::LPR;
+    static_assert(L::kStageTableLen <= N, "the per-stage twiddle table fits its region");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T>* X = reinterpret_cast<cx<T>*>(smem_raw);
     cx<T>* Sx = reinterpret_cast<cx<T>*>(smem_raw + S_::XB);
@@ -178,18 +185,42 @@ __global__ void __launch_bounds__(PlaneShape<T, N, RA, RB, P, RC>::THREADS, 2)
 
     // the tables this pass reads per element, staged once (they do not depend
     // on the state, so before the wait on the previous kernel)
-    {
-        const float4* tg = reinterpret_cast<const float4*>(a.tw);
-        for (int i = tid; i < N; i += S_::THREADS) {
-            tws[i] = __ldg(tg + i);
-            dx_s[i] = a.vd[0][i];
-            dy_s[i] = a.vd[1][i];
-        }
+    L::build_stage_table(tws, reinterpret_cast<const float4*>(a.tw), tid, S_::THREADS);
+    for (int i = tid; i < N; i += S_::THREADS) {
+        dx_s[i] = a.vd[0][i];
+        dy_s[i] = a.vd[1][i];
     }
-    if (tid == 0) mbar_init(bar, 1);
+    if (tid == 0) {
+        mbar_init(bar, 1);      // rows 0..15 (into S)
+        mbar_init(bar + 1, 1);  // rows 16..31 (into X)
+    }
     __syncthreads();
     const cx<T>* twp = reinterpret_cast<const cx<T>*>(tws);
     pdl_wait();
+
+    const unsigned row_bytes = (unsigned)(N * sizeof(cx<T>));
+    // rows [r0, r0 + 16) of this CTA's slice of plane z land in `dst` at a
+    // line stride of `stride` elements, completing on mbarrier b; the first
+    // warp issues one bulk copy per row
+    auto land_rows = [&](long z, int r0, cx<T>* dst, int stride, uint64_t* b) {
+        if (tid < 32) {
+            // order earlier generic-proxy accesses to dst before the bulk
+            // copies (async proxy) that overwrite it
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            if (tid == 0)
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                             ::"r"(smem_addr(b)), "r"(row_bytes * LPR) : "memory");
+            __syncwarp();
+            if (tid < LPR) {
+                const cx<T>* src = in + (size_t)z * plane + (size_t)(rank * RPC + r0 + tid) * N;
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], "
+                    "[%1], %2, [%3];" ::"r"(smem_addr(dst + tid * stride)),
+                    "l"(src), "r"(row_bytes), "r"(smem_addr(b))
+                    : "memory");
+            }
+        }
+    };
 
     // row phase: thread rt of line rl (rows rl and LPR + rl); column phase:
     // thread ct of column cc (columns cc and LPR + cc of this CTA's 32)
@@ -198,42 +229,30 @@ __global__ void __launch_bounds__(PlaneShape<T, N, RA, RB, P, RC>::THREADS, 2)
     auto row_sync = [] { __syncwarp(); };
     auto col_sync = [] { __syncthreads(); };
     const unsigned x_addr = smem_addr(X);
-    const unsigned row_bytes = (unsigned)(N * sizeof(cx<T>));
 
     KSum acc{0.0, 0.0};
     bool ok = true;
-    unsigned parity = 0;
+    unsigned par0 = 0, par1 = 0;
+    long z = cluster_index();
+    if (z < nz) land_rows(z, 0, Sx, S_::SLS, bar);
     cluster_arrive();  // X is free (pairs with the first wait below)
-    for (long z = cluster_index(); z < nz; z += zstep) {
+    for (; z < nz; z += zstep) {
         cluster_wait();  // the cluster has finished reading the previous plane's X
-        // this CTA's 32 rows of plane z land in X, one bulk copy per row slot
-        if (tid < 32) {
-            // order the generic-proxy accesses to X before the bulk copies
-            // (async proxy) that overwrite it
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            if (tid == 0)
-                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
-                             ::"r"(smem_addr(bar)), "r"(row_bytes * RPC) : "memory");
-            __syncwarp();
-            const cx<T>* src = in + (size_t)z * plane + (size_t)(rank * RPC + tid) * N;
-            asm volatile(
-                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], "
-                "%2, [%3];" ::"r"(smem_addr(X + tid * S_::LSR)),
-                "l"(src), "r"(row_bytes), "r"(smem_addr(bar))
-                : "memory");
-        }
-        ok &= mbar_wait(bar, parity, kPlaneWaitPolls);
-        parity ^= 1u;
+        if constexpr (LPR < RPC) land_rows(z, LPR, X + LPR * S_::LSR, S_::LSR, bar + 1);
 
-        // ---- row phase (x lines), two rounds of LPR rows
+        // ---- row phase (x lines): rows 0..15 from S, then rows 16..31 from
+        // their X slots; the transforms exchange through S
         const double sc = (!INV && a.ops[0]) ? *a.scale_in : 1.0;
 #pragma unroll 1
         for (int rd = 0; rd < RPC / LPR; ++rd) {
             const int row = rd * LPR + rl;
             cx<T>* xr = X + row * S_::LSR;
+            const cx<T>* src = rd == 0 ? Sx + rl * S_::SLS : xr;
+            ok &= mbar_wait(bar + rd, rd == 0 ? par0 : par1, kPlaneWaitPolls);
             cx<T> v[E];
 #pragma unroll
-            for (int e = 0; e < E; ++e) v[e] = xr[L::index(rt, e)];
+            for (int e = 0; e < E; ++e) v[e] = src[L::index(rt, e)];
+            __syncthreads();  // every row's landed values are in registers
             cx<T>* srow = Sx + rl * S_::SLS;
             if constexpr (!INV) {
                 const int y = (int)rank * RPC + row;
@@ -250,11 +269,11 @@ __global__ void __launch_bounds__(PlaneShape<T, N, RA, RB, P, RC>::THREADS, 2)
 #pragma unroll
                 for (int e = 0; e < E; ++e) v[e].y = -v[e].y;
             }
-            // the row's threads have read its landed values (the transform
-            // synchronised them), so its slot takes the padded output
 #pragma unroll
             for (int e = 0; e < E; ++e) xr[smem_phys(L::index(rt, e))] = v[e];
         }
+        par0 ^= 1u;
+        if constexpr (LPR < RPC) par1 ^= 1u;
         cluster_arrive();
         cluster_wait();  // every CTA's X holds this plane's rows
 
@@ -272,14 +291,18 @@ __global__ void __launch_bounds__(PlaneShape<T, N, RA, RB, P, RC>::THREADS, 2)
                     x_addr + (unsigned)(((y % RPC) * S_::LSR + col_off) * (int)sizeof(cx<T>));
                 v[e] = dsmem_load<T>(dsmem_map(la, (unsigned)(y / RPC)));
             }
-            if (rd == RPC / LPR - 1) cluster_arrive();  // done reading X
+            const bool last = rd == RPC / LPR - 1;
+            if (last) cluster_arrive();  // done reading X
             cx<T>* scol = Sx + cc * S_::LSC;
-            if constexpr (!INV) {
-                L::template forward<true>(v, ct, scol, twp, col_sync);
-            } else {
+            if constexpr (INV) {
 #pragma unroll
                 for (int e = 0; e < E; ++e) v[e].y = -v[e].y;
-                L::template forward<true>(v, ct, scol, twp, col_sync);
+            }
+            L::template forward<true>(v, ct, scol, twp, col_sync);
+            // S is free again (the transform ends with a block barrier): the
+            // next plane's first rows land there while this one finishes
+            if (last && z + zstep < nz) land_rows(z + zstep, 0, Sx, S_::SLS, bar);
+            if constexpr (INV) {
 #pragma unroll
                 for (int e = 0; e < E; ++e) v[e].y = -v[e].y;
                 const cx<double> lf = cmul(ld2(a.vfac[0], x_col), ld2(a.vfac[2], (int)z));
