@@ -1,27 +1,32 @@
 #!/usr/bin/env python
 """Benchmark of the split-operator Gross-Pitaevskii step on B200.
 
-Workload (the configuration the headline metric is quoted on): a 2D real-time
-rotating condensate, 1024^2 grid on [-16,16)^2, hbar = m = 1, wx = wy = 1,
-g = 500, rotation Omega = 0.7 as the gauge A = Omega(-y, x) applied by
-per-axis 1D FFT passes, dt = 5e-5.  The initial state is a seeded synthetic
-stand-in for "the FP64 ground state with a smoothed random phase": an FP64
-imaginary-time relaxation of the same Hamiltonian on the GPU (done before
-timing) times exp(i theta), theta = 2 pi U(0,1) smoothed by a Gaussian of width
-0.5 (seed 2).
+Headline workload: the 3D imaginary-time ground state on a 256^3 grid on
+[-12,12)^3, hbar = m = 1, anisotropic trap (wx, wy, wz) = (1, 1, 4), g = 1000,
+dt = 1e-4, renormalised every step, from a seeded Gaussian of width 1 times
+(1 + 0.01 xi), xi ~ N(0,1) iid (PCG64 seed 3), normalised.  It is the largest
+configuration that fits one GPU and the one the ground-state accuracy gate
+(dE/E <= 1e-6 against the FP64 form) applies to.  The field (128 MiB complex64,
+256 MiB complex128) is larger than L2 (126 MB), so no flush is needed between
+timed steps.
 
-One bench step = one gpue_evolve call of 100 split-operator time steps
-(GPUE's default printSteps segment, an even number so both x/y gauge orders
-occur equally), run by the fused complex64 form through the C ABI.  L2
-(126 MB) is flushed by a 256 MiB write before every timed step; each step is
+One bench step = one gpue_evolve call of 100 imaginary time steps of the fused
+complex64 form through the C ABI (three full-field passes per time step: the
+XY-plane pass, the z pass with the kinetic phase, the inverse XY-plane pass),
 timed with CUDA events on the library's stream.  The same protocol times the
-plain FP64 form for the fused-FP32 vs plain-FP64 ratio.
+plain FP64 form (five line passes per step) for the fused-FP32 vs plain-FP64
+ratio.  Extra legs: end to end through the C ABI with host buffers, the full
+5000-step relaxation per form with its energies, the 1024^2 rotating
+real-time case, the 256^2 FP64 ground state (10,000 steps), the 96-solve
+batched sweep and the serving stream.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
 --impl reference times GPUE's path on the host CPU: the reference has no CPU
 implementation, so this arm runs the FP64 CPU restatement of it (oracle/,
-OpenMP over all host threads) on the same workload.
+OpenMP over all host threads) on the same workload from the same initial
+state; when GPUE's own CUDA build is present (oracle/_ref) the arm also times
+it on this GPU on the full-size configurations, as an extra key.
 """
 
 import argparse
@@ -30,6 +35,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -40,31 +46,67 @@ from gpue_b200 import replicas  # noqa: E402  (pure Python; loads no library)
 METRIC = ("grid-point-steps/s fused-FP32 vs plain-FP64 (same B200, ΔE/E≤1e-6); "
           "p99 lat")
 UNIT = "grid-point-steps/s"
-WORK = dict(dim=2, n=1024, box=16.0, wx=1.0, wy=1.0, g=500.0, omega=0.7, gauge=True,
-            dt=5e-5, gdt=1e-4, total_steps=20000)
-WORKLOAD_NAME = ("2D real-time rotating condensate 1024^2 on [-16,16)^2, g=500, Omega=0.7 "
-                 "gauge, dt=5e-5")
+HEAD = dict(dim=3, n=256, box=12.0, wz=4.0, g=1000.0, gdt=1e-4, total_steps=5000,
+            polish=50, seed=3)
+WORKLOAD_NAME = ("3D imaginary-time ground state 256^3 on [-12,12)^3, (wx,wy,wz)=(1,1,4), "
+                 "g=1000, dt=1e-4, renormalised every step")
 STEPS_PER_BENCH_STEP = 100
+REF_STEPS_PER_BENCH_STEP = 4  # the CPU arm's bench step (about a second of host work)
+# the 1024^2 rotating real-time case (extra leg)
+ROT = dict(dim=2, n=1024, box=16.0, g=500.0, omega=0.7, dt=5e-5, gdt=1e-4, total_steps=20000)
+ROT_NAME = ("2D real-time rotating condensate 1024^2 on [-16,16)^2, g=500, Omega=0.7 gauge, "
+            "dt=5e-5")
+# the 256^2 plain FP64 ground state (extra leg)
+SMALL = dict(dim=2, n=256, box=10.0, g=100.0, gdt=1e-4, steps=10000, every=1000, seed=1)
 FLUSH_BYTES = 256 << 20
+# passes per time step of each form on the headline workload
+PASSES = {"fp32": 3, "fp64": 5}
 
 
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--quick", action="store_true", help="skip the steady-state and e2e legs")
-    ap.add_argument("--only", choices=["batch", "serve", "large"], default=None,
-                    help="run one auxiliary leg alone and print its JSON")
+    ap.add_argument("--quick", action="store_true", help="headline and e2e only")
+    ap.add_argument("--only", choices=["batch", "serve", "accuracy", "rot2d", "small2d"],
+                    default=None, help="run one auxiliary leg alone and print its JSON")
     ap.add_argument("--profile", choices=["fp32", "fp64", "fp32_3d", "fp64_3d"], default=None,
-                    help="profiling case for ncu: the same workload without the relaxation "
-                         "prep, --warmup + --steps time steps of one form, no timing output")
+                    help="profiling case for ncu: --warmup + --steps time steps of one form "
+                         "(3D: the headline workload; 2D: the rotating case), no timing output")
     return ap.parse_args()
 
 
 # ----------------------------------------------------------- inputs -------
+
+def gauss_start(dim, n, box, seed, normalise=False):
+    """exp(-r^2/2) (1 + 0.01 xi), xi ~ N(0,1) iid (PCG64 seed), complex128,
+    optionally normalised to sum |psi|^2 dV = 1."""
+    import numpy as np
+    dx = box / (n >> 1)
+    x = -box + dx * np.arange(n)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    if dim == 2:
+        r2 = x[None, :] ** 2 + x[:, None] ** 2
+    else:
+        r2 = x[None, None, :] ** 2 + x[None, :, None] ** 2 + x[:, None, None] ** 2
+    psi = np.exp(-r2 / 2.0) * (1.0 + 0.01 * rng.standard_normal(r2.shape))
+    psi = psi.astype(np.complex128)
+    if normalise:
+        psi /= np.sqrt(np.sum(np.abs(psi) ** 2) * dx ** dim)
+    return psi
+
+
+def head_state():
+    return gauss_start(3, HEAD["n"], HEAD["box"], HEAD["seed"], normalise=True)
+
+
+def head_params(G, precision, device=0):
+    return G.make_params(3, HEAD["n"], HEAD["box"], wz=HEAD["wz"], g=HEAD["g"],
+                         gdt=HEAD["gdt"], precision=precision, device=device)
+
 
 def phase_field(n, box, seed=2):
     import numpy as np
@@ -76,16 +118,16 @@ def phase_field(n, box, seed=2):
     return np.real(np.fft.ifft2(np.fft.fft2(theta) * np.exp(-0.5 * k2 * 0.25)))
 
 
-def initial_state(G, device):
+def rot_state(G, device):
     """FP64 imaginary-time relaxation (GPU) times a smoothed random phase."""
     import numpy as np
-    n, box = WORK["n"], WORK["box"]
+    n, box = ROT["n"], ROT["box"]
     dx = box / (n >> 1)
     x = -box + dx * np.arange(n)
     r2 = x[None, :] ** 2 + x[:, None] ** 2
     psi = np.exp(-r2 / 8.0).astype(np.complex128)
-    p = G.make_params(2, n, box, g=WORK["g"], omega=WORK["omega"], gauge=True, gdt=2e-3,
-                      dt=WORK["dt"], precision=G.PREC_FP64, device=device)
+    p = G.make_params(2, n, box, g=ROT["g"], omega=ROT["omega"], gauge=True, gdt=2e-3,
+                      dt=ROT["dt"], precision=G.PREC_FP64, device=device)
     with G.Solver(p) as s:
         s.set_wfc(psi)
         s.evolve(5000, 0)
@@ -93,10 +135,9 @@ def initial_state(G, device):
     return np.ascontiguousarray(gs * np.exp(1j * phase_field(n, box)))
 
 
-def work_params(G, precision, device):
-    return G.make_params(2, WORK["n"], WORK["box"], wx=WORK["wx"], wy=WORK["wy"],
-                         g=WORK["g"], omega=WORK["omega"], gauge=True, gdt=WORK["gdt"],
-                         dt=WORK["dt"], precision=precision, device=device)
+def rot_params(G, precision, device):
+    return G.make_params(2, ROT["n"], ROT["box"], g=ROT["g"], omega=ROT["omega"], gauge=True,
+                         gdt=ROT["gdt"], dt=ROT["dt"], precision=precision, device=device)
 
 
 # ------------------------------------------------------------ clocks ------
@@ -169,15 +210,18 @@ class ClockSampler:
 
 # ------------------------------------------------------- GPU timing -------
 
-def timed_steps(G, torch, s, steps, warmup, dev, flush, barrier, sampler=None):
-    """Per bench step: flush L2, then one 100-time-step evolve between CUDA events."""
+def timed_steps(G, torch, s, steps, warmup, dev, barrier, gstate, flush=None, sampler=None):
+    """Per bench step one gpue_evolve call of STEPS_PER_BENCH_STEP time steps
+    between CUDA events on the library's stream (after an L2 flush when
+    `flush` is given)."""
     stream = torch.cuda.ExternalStream(s.stream(), device=dev)
     launches = 0
     off = 0
     for _ in range(warmup):
-        with torch.cuda.stream(stream):
-            flush.fill_(1)
-        s.evolve(STEPS_PER_BENCH_STEP, 1, no_sync=True, step_offset=off)
+        if flush is not None:
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+        s.evolve(STEPS_PER_BENCH_STEP, gstate, no_sync=True, step_offset=off)
         off += STEPS_PER_BENCH_STEP
     torch.cuda.synchronize(dev)
     barrier()
@@ -189,9 +233,10 @@ def timed_steps(G, torch, s, steps, warmup, dev, flush, barrier, sampler=None):
         sampler.mark(0)
     for k in range(steps):
         with torch.cuda.stream(stream):
-            flush.fill_(float(k & 7))
+            if flush is not None:
+                flush.fill_(float(k & 7))
             ev[k][0].record(stream)
-        r = s.evolve(STEPS_PER_BENCH_STEP, 1, no_sync=True, step_offset=off)
+        r = s.evolve(STEPS_PER_BENCH_STEP, gstate, no_sync=True, step_offset=off)
         launches += r["kernel_launches"]
         off += STEPS_PER_BENCH_STEP
         with torch.cuda.stream(stream):
@@ -206,68 +251,126 @@ def timed_steps(G, torch, s, steps, warmup, dev, flush, barrier, sampler=None):
     return ms, launches, clocks
 
 
-def steady_state(G, s, nsteps):
-    """One gpue_evolve call of nsteps (graph-replayed, no flushes)."""
-    r = s.evolve(nsteps, 1)
-    return r["device_ms"], r["kernel_launches"]
-
-
-def e2e_leg(G, torch, psi0, dev, calls=10, steps_per_call=100, dist=None):
-    """Through the C ABI with pinned host buffers: upload psi (complex128),
-    evolve one printSteps-sized segment, download psi and the energy."""
-    import numpy as np
-    n = WORK["n"]
-    pin_in = torch.empty((n, n), dtype=torch.complex128, pin_memory=True)
-    pin_out = torch.empty((n, n), dtype=torch.complex128, pin_memory=True)
+def e2e_leg(G, torch, psi0, dev, calls=5, dist=None):
+    """Through the C ABI with pinned host buffers on the headline workload:
+    upload psi (complex128), evolve one bench step (100 imaginary time steps,
+    fused complex64), download psi (complex128) and the energy."""
+    import ctypes as C
+    shape = psi0.shape
+    pin_in = torch.empty(shape, dtype=torch.complex128, pin_memory=True)
+    pin_out = torch.empty(shape, dtype=torch.complex128, pin_memory=True)
     hin = pin_in.numpy()
     hin[...] = psi0
     hout = pin_out.numpy()
-    import ctypes as C
-    with G.Solver(work_params(G, G.PREC_FP32, dev)) as s:
+    with G.Solver(head_params(G, G.PREC_FP32, dev)) as s:
         stream = torch.cuda.ExternalStream(s.stream(), device=dev)
         L = G.lib()
         # warm the graphs once
         L.gpue_set_wfc(s._h, C.c_void_p(hin.ctypes.data), G.MEM_HOST, G.C128)
-        s.evolve(steps_per_call, 1)
+        s.evolve(STEPS_PER_BENCH_STEP, 0)
         torch.cuda.synchronize(dev)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with torch.cuda.stream(stream):
             e0.record(stream)
-        energies = []
         off = 0
         for _ in range(calls):
             assert L.gpue_set_wfc(s._h, C.c_void_p(hin.ctypes.data), G.MEM_HOST, G.C128) == 0
-            s.evolve(steps_per_call, 1, no_sync=True, step_offset=off)
-            off += steps_per_call
+            s.evolve(STEPS_PER_BENCH_STEP, 0, no_sync=True, step_offset=off)
+            off += STEPS_PER_BENCH_STEP
             assert L.gpue_get_wfc(s._h, C.c_void_p(hout.ctypes.data), G.MEM_HOST, G.C128) == 0
-            energies.append(s.energy())
+            s.energy()
         with torch.cuda.stream(stream):
             e1.record(stream)
         torch.cuda.synchronize(dev)
         ms = e0.elapsed_time(e1)
-    pts = n * n
-    rate, _, secs = replicas.job_rate(pts * steps_per_call * calls, ms * 1e-3, dist, dev)
-    ms = secs * 1e3
+    pts = psi0.size
+    rate, _, secs = replicas.job_rate(pts * STEPS_PER_BENCH_STEP * calls, ms * 1e-3, dist, dev)
     return {"value": rate, "unit": UNIT,
             "h2d_bytes_per_step": pts * 16, "d2h_bytes_per_step": pts * 16 + 8,
-            "step": "one gpue_evolve() call of %d time steps (GPUE's default printSteps) "
-                    "with psi uploaded from pinned host memory before it and psi plus the "
-                    "energy read back after it" % steps_per_call,
-            "calls": calls, "ms": ms}
+            "step": "one gpue_evolve() call of %d imaginary time steps with psi uploaded "
+                    "from pinned host memory (complex128) before it and psi (complex128) "
+                    "plus the energy read back after it" % STEPS_PER_BENCH_STEP,
+            "calls": calls, "ms": secs * 1e3}
 
 
-def accuracy_leg(G, psi0, dev, nsteps=2000):
-    """Energy drift of the fused FP32 form against the plain FP64 form over
-    nsteps real-time steps from the same state (the FP64 form is pinned to
-    GPUE's own build by the parity tests)."""
-    out = {}
+def accuracy_leg(G, dev, peak):
+    """The full relaxation of the headline workload per form: 5000 imaginary
+    time steps (steady state, graph-replayed) and the energies, then 50 FP64
+    polish steps on both; the FP64 form is pinned to GPUE's own build."""
+    psi0 = head_state()
+    pts = HEAD["n"] ** 3
+    out = {"workload": WORKLOAD_NAME + ", %d steps (+%d FP64 polish steps)"
+           % (HEAD["total_steps"], HEAD["polish"])}
+    res = {}
     for name, prec in (("fp64", G.PREC_FP64), ("fp32", G.PREC_FP32)):
-        with G.Solver(work_params(G, prec, dev)) as s:
+        with G.Solver(head_params(G, prec, dev)) as s:
+            s.autotune()
             s.set_wfc(psi0)
-            s.evolve(nsteps, 1)
-            out[name] = s.energy()
-    return {"steps": nsteps, "E_fp64": out["fp64"], "E_fp32": out["fp32"],
-            "dE_rel": abs(out["fp32"] - out["fp64"]) / abs(out["fp64"])}
+            r = s.evolve(HEAD["total_steps"], 0)
+            E = s.energy()
+            if name == "fp64":
+                s.evolve(HEAD["polish"], 0, step_offset=HEAD["total_steps"])
+            else:
+                s.evolve(0, 0, polish_steps=HEAD["polish"], step_offset=HEAD["total_steps"])
+            res[name] = (r["device_ms"] * 1e-3 / HEAD["total_steps"], E, s.energy())
+    t64, E64, E64p = res["fp64"]
+    t32, E32, E32p = res["fp32"]
+    out.update({
+        "fp32_value": pts / t32, "fp64_value": pts / t64, "unit": UNIT,
+        "fp32_over_fp64": t64 / t32,
+        "E_fp64": E64, "E_fp32": E32, "dE_rel_fp32": abs(E32 - E64) / abs(E64),
+        "E_fp64_polished": E64p, "E_fp32_polished": E32p,
+        "dE_rel_fp32_polished": abs(E32p - E64p) / abs(E64p),
+        "alg_frac_80B": 80 * pts / t32 / 1e9 / peak,
+        "note": "steady-state device time of one gpue_evolve call of 5000 steps per form; "
+                "alg_frac_80B = 80 bytes per point and step (five full-field complex64 "
+                "read+write passes, the line schedule) x points/s over the measured HBM "
+                "copy rate"})
+    return out
+
+
+def rot2d_leg(G, torch, dev, barrier, steps=20, warmup=3):
+    """The 1024^2 rotating real-time case: flushed bench steps per form."""
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    psi0 = rot_state(G, dev)
+    pts = ROT["n"] ** 2
+    out = {"workload": ROT_NAME}
+    for name, prec in (("fp64", G.PREC_FP64), ("fp32", G.PREC_FP32)):
+        with G.Solver(rot_params(G, prec, dev)) as s:
+            s.autotune()
+            s.set_wfc(psi0)
+            ms, _, _ = timed_steps(G, torch, s, steps, warmup, dev, barrier, 1, flush=flush)
+            r = s.evolve(ROT["total_steps"], 1)
+        out[name + "_value"] = pts * steps * STEPS_PER_BENCH_STEP / (ms * 1e-3)
+        out[name + "_steady_value"] = pts * ROT["total_steps"] / (r["device_ms"] * 1e-3)
+    out["fp32_over_fp64"] = out["fp32_value"] / out["fp64_value"]
+    out["unit"] = UNIT
+    out["note"] = ("value: %d flushed bench steps of %d real-time steps; steady: one "
+                   "gpue_evolve call of %d steps, graph-replayed"
+                   % (steps, STEPS_PER_BENCH_STEP, ROT["total_steps"]))
+    return out
+
+
+def small2d_leg(G, dev):
+    """The 256^2 ground state on [-10,10)^2, g = 100, dt = 1e-4, 10,000 steps
+    with energy checks every 1000: one gpue_evolve call per form."""
+    psi0 = gauss_start(2, SMALL["n"], SMALL["box"], SMALL["seed"], normalise=True)
+    pts = SMALL["n"] ** 2
+    out = {"workload": "2D imaginary-time ground state 256^2 on [-10,10)^2, g=100, dt=1e-4, "
+                       "10000 steps, renormalised every step"}
+    for name, prec in (("fp64", G.PREC_FP64), ("fp32", G.PREC_FP32)):
+        with G.Solver(G.make_params(2, SMALL["n"], SMALL["box"], g=SMALL["g"],
+                                    gdt=SMALL["gdt"], precision=prec, device=dev)) as s:
+            s.autotune()
+            s.set_wfc(psi0)
+            s.evolve(SMALL["every"], 0)  # graphs
+            s.set_wfc(psi0)
+            r = s.evolve(SMALL["steps"], 0, energy_every=SMALL["every"])
+            out[name + "_value"] = pts * SMALL["steps"] / (r["device_ms"] * 1e-3)
+            out[name + "_energy"] = s.energy()
+            out[name + "_us_per_step"] = r["device_ms"] * 1e3 / SMALL["steps"]
+    out["unit"] = UNIT
+    return out
 
 
 # ------------------------------------------------- batched sweep ----------
@@ -279,20 +382,6 @@ BATCH = dict(solves=96, sizes=(128, 192, 256, 384, 512), box=10.0, gdt=1e-4, eve
              thr=1e-10, seed=4)
 # the sample timed: steps 0..1000 (checks at 0, 100, ..., 1000) of every solve
 BATCH_STEPS = 1001
-
-
-def gauss_start(dim, n, box, seed):
-    """exp(-r^2/2) (1 + 0.01 xi), xi ~ N(0,1) iid (PCG64 seed), complex128."""
-    import numpy as np
-    dx = box / (n >> 1)
-    x = -box + dx * np.arange(n)
-    rng = np.random.Generator(np.random.PCG64(seed))
-    if dim == 2:
-        r2 = x[None, :] ** 2 + x[:, None] ** 2
-    else:
-        r2 = x[None, None, :] ** 2 + x[None, :, None] ** 2 + x[:, None, None] ** 2
-    psi = np.exp(-r2 / 2.0) * (1.0 + 0.01 * rng.standard_normal(r2.shape))
-    return psi.astype(np.complex128)
 
 
 def batch_cases():
@@ -356,62 +445,6 @@ def batch_leg(G, dev, steps=BATCH_STEPS, dist=None):
                       "absolute stop; none is expected to stop this early), complex64 with "
                       "FP64 reductions; sequential = the same solves through gpue_evolve one "
                       "after another (sum of their device times)" % (steps - 1)}
-
-
-# ---------------------------------------------------- large 3D ground state
-
-# 256^3 on [-12,12)^3, (wx,wy,wz) = (1,1,4), g = 1000, dt = 1e-4, 5000
-# imaginary-time steps from a Gaussian of width 1 times (1 + 0.01 xi) (seed
-# 3); the fused form then polishes with 50 FP64 steps.  The field (128 MiB
-# complex64, 256 MiB complex128) does not fit in L2, so this is the case the
-# HBM roofline describes.
-LARGE = dict(n=256, box=12.0, wz=4.0, g=1000.0, gdt=1e-4, steps=5000, polish=50, seed=3)
-
-
-def large_leg(G, dev, peak):
-    n = LARGE["n"]
-    psi0 = gauss_start(3, n, LARGE["box"], LARGE["seed"])
-    pts = n ** 3
-    out = {"workload": "3D imaginary-time ground state 256^3 on [-12,12)^3, (1,1,4) trap, "
-                       "g=1000, dt=1e-4, 5000 steps (+50 FP64 polish steps for the fused form)"}
-
-    def params(prec):
-        return G.make_params(3, n, LARGE["box"], wz=LARGE["wz"], g=LARGE["g"], gdt=LARGE["gdt"],
-                             precision=prec, device=dev)
-
-    with G.Solver(params(G.PREC_FP64)) as s:
-        plans64 = s.autotune()
-        s.set_wfc(psi0)
-        r = s.evolve(LARGE["steps"], 0)
-        E64 = s.energy()
-        s.evolve(LARGE["polish"], 0, step_offset=LARGE["steps"])
-        E64p = s.energy()
-    t64 = r["device_ms"] * 1e-3 / LARGE["steps"]
-    with G.Solver(params(G.PREC_FP32)) as s:
-        plans32 = s.autotune()
-        s.set_wfc(psi0)
-        r = s.evolve(LARGE["steps"], 0)
-        E32 = s.energy()
-        s.evolve(0, 0, polish_steps=LARGE["polish"], step_offset=LARGE["steps"])
-        E32p = s.energy()
-    t32 = r["device_ms"] * 1e-3 / LARGE["steps"]
-    # 5 full-field read+write passes per 3D step (no gauge): 2*5*s bytes per point
-    out.update({
-        "fp32_value": pts / t32, "fp64_value": pts / t64, "unit": UNIT,
-        "fp32_over_fp64": t64 / t32,
-        "fp32_roofline_frac": 2 * 5 * 8 * pts / t32 / 1e9 / peak,
-        "fp64_roofline_frac": 2 * 5 * 16 * pts / t64 / 1e9 / peak,
-        "E_fp64": E64, "E_fp32": E32, "dE_rel_fp32": abs(E32 - E64) / abs(E64),
-        "E_fp64_5050": E64p, "E_fp32_polished": E32p,
-        "dE_rel_fp32_polished": abs(E32p - E64p) / abs(E64p),
-        "plans_fp32": [(p["ra"], p["rb"], p["threads_per_line"], p["lines_per_cta"])
-                       for p in plans32],
-        "plans_fp64": [(p["ra"], p["rb"], p["threads_per_line"], p["lines_per_cta"])
-                       for p in plans64],
-        "note": "steady-state device time of one gpue_evolve call of 5000 steps per form "
-                "(graph-replayed, renormalised every step); roofline bytes 2*5*8 (complex64) "
-                "or 2*5*16 (complex128) per point and step against the measured HBM copy rate"})
-    return out
 
 
 # -------------------------------------------------------------- serving ---
@@ -519,66 +552,116 @@ def serve_leg(G, dev):
 
 # ------------------------------------------------------------- CPU --------
 
-def cpu_oracle_rate(psi0, budget_s=12.0, threads=0):
-    """FP64 CPU restatement (oracle) on the same workload, bounded sample."""
+def cpu_oracle_rate(psi0, budget_s=15.0, threads=0):
+    """FP64 CPU restatement (oracle) on the headline workload from the same
+    initial state: a bounded sample of imaginary time steps."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    n = WORK["n"]
-    P = oracle.Problem(2, n, WORK["box"], g=WORK["g"], omega=WORK["omega"], gauge=True,
-                       dt=WORK["dt"], gdt=WORK["gdt"], threads=threads)
+    n = HEAD["n"]
+    P = oracle.Problem(3, n, HEAD["box"], wz=HEAD["wz"], g=HEAD["g"], gdt=HEAD["gdt"],
+                       threads=threads)
     t = time.time()
-    P.evolve(psi0, 2, 1)
-    per = (time.time() - t) / 2
-    steps = max(2, min(2000, int(budget_s / max(per, 1e-6))))
-    steps += steps % 2
+    psi, _, _ = P.evolve(psi0, 1, 0)
+    per = time.time() - t
+    steps = max(1, min(50, int(budget_s / max(per, 1e-6))))
     t = time.time()
-    P.evolve(psi0, steps, 1)
+    P.evolve(psi, steps, 0)
     dt = time.time() - t
     cores = threads or os.cpu_count()
-    return {"value": n * n * steps / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": "%d real-time steps of the 1024^2 rotating case (FP64, OpenMP over "
-                      "lines, %d threads)" % (steps, cores), "seconds": dt}
+    return {"value": n ** 3 * steps / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "%d imaginary time steps of the 256^3 ground state from the headline's "
+                      "initial state (FP64, OpenMP over lines, %d threads)" % (steps, cores),
+            "seconds": dt}
+
+
+def gpue_cuda_build_leg():
+    """GPUE's own CUDA build (oracle/_ref, compiled from the reference sources)
+    timed on this GPU by its harness: evolve() on the full-size workloads with
+    the step counts below, GPUE's per-step device-to-host copy of psi included
+    as GPUE does it.  None when the build is absent."""
+    harness = os.path.join(ROOT, "oracle", "_ref", "gpue_ref_harness")
+    if not os.path.exists(harness):
+        return {"unavailable": "oracle/_ref/gpue_ref_harness not built"}
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import numpy as np
+    import cases
+    out = {}
+    for name, steps in (("cfg3_256_imag", 100), ("cfg2_1024_real_gauge", 1000),
+                        ("cfg1_256_imag", 10000)):
+        c = cases.case(name)
+        c["gsteps" if c["gsteps"] else "esteps"] = steps
+        c["energy_every"] = 0
+        psi0 = cases.initial_psi(c)
+        with tempfile.TemporaryDirectory() as td:
+            p0 = os.path.join(td, "psi0.bin")
+            psi0.tofile(p0)
+            prefix = os.path.join(td, "out")
+            r = subprocess.run([harness] + cases.harness_args(c, p0, prefix,
+                                                              os.path.join(td, "d")),
+                               stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True,
+                               timeout=600)
+            if r.returncode != 0:
+                out[name] = {"failed": r.stdout[-300:]}
+                continue
+            phase = "imag" if c["gsteps"] > 0 else "real"
+            info = dict(l.split() for l in open(prefix + "_%s.txt" % phase))
+        secs = float(info["evolve_s"])
+        pts = c["n"] ** c["dim"]
+        out[name] = {"steps": steps, "evolve_s": secs,
+                     "value": pts * steps / secs, "unit": UNIT,
+                     "energy": float(info["energy"])}
+        del psi0
+    out["note"] = ("GPUE's build (FP64, cuFFT) timed by its harness around evolve(); "
+                   "cfg3 = the headline 256^3 workload, cfg2 = the 1024^2 rotating case, "
+                   "cfg1 = the 256^2 ground state")
+    _ = np
+    return out
 
 
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import numpy as np
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    n = WORK["n"]
-    dx = WORK["box"] / (n >> 1)
-    x = -WORK["box"] + dx * np.arange(n)
-    psi0 = (np.exp(-(x[None, :] ** 2 + x[:, None] ** 2) / 8.0) *
-            np.exp(1j * phase_field(n, WORK["box"]))).astype(np.complex128)
-    psi0 /= np.sqrt(np.sum(abs(psi0) ** 2) * dx * dx)
     import oracle
-    P = oracle.Problem(2, n, WORK["box"], g=WORK["g"], omega=WORK["omega"], gauge=True,
-                       dt=WORK["dt"], gdt=WORK["gdt"])
+    n = HEAD["n"]
+    psi0 = head_state()
+    P = oracle.Problem(3, n, HEAD["box"], wz=HEAD["wz"], g=HEAD["g"], gdt=HEAD["gdt"])
     budget = 150.0
+    per = REF_STEPS_PER_BENCH_STEP
     psi = psi0
-    for _ in range(min(args.warmup, 2)):
-        psi, _, _ = P.evolve(psi, STEPS_PER_BENCH_STEP, 1)
+    # one reference bench step = one evolve call of `per` imaginary time steps
+    # of the headline workload
+    for _ in range(min(args.warmup, 1)):
+        psi, _, _ = P.evolve(psi, per, 0)
     t0 = time.time()
     done = 0
     while done < args.steps and time.time() - t0 < budget:
-        psi, _, _ = P.evolve(psi, STEPS_PER_BENCH_STEP, 1)
+        psi, _, _ = P.evolve(psi, per, 0)
         done += 1
     secs = time.time() - t0
-    val = n * n * STEPS_PER_BENCH_STEP * done / secs
+    val = n ** 3 * per * done / secs
     cores = os.cpu_count()
     line = {"metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
             "steps": done, "warmup": args.warmup, "ms_per_step": 1e3 * secs / max(done, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded)", "impl": "reference",
-            "config": {"workload": WORKLOAD_NAME, "grid": n, "step": "2 time steps",
-                       "steps_requested": args.steps, "budget_s": budget},
+            "data": "synthetic (seeded; the headline's initial state)", "impl": "reference",
+            "config": {"workload": WORKLOAD_NAME, "grid": n,
+                       "step": "one evolve call of %d imaginary time steps (the reference "
+                               "arm's bench step; points x time steps / seconds is the same "
+                               "metric)" % per,
+                       "steps_requested": args.steps, "budget_s": budget,
+                       "initial_state": "the headline's (seed 3 Gaussian, normalised)"},
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": "%d bench steps (%d time steps) of the same workload "
+                             "sample": "%d imaginary time steps of the headline workload "
                                        "on the FP64 CPU restatement, OpenMP over %d threads"
-                                       % (done, done * STEPS_PER_BENCH_STEP, cores)},
+                                       % (done * per, cores)},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
+    try:
+        line["gpue_cuda_build"] = gpue_cuda_build_leg()
+    except Exception as e:  # the CPU arm stands without it
+        line["gpue_cuda_build"] = {"unavailable": str(e)[:200]}
     print(json.dumps(line), flush=True)
 
 
@@ -594,35 +677,33 @@ def measured_peak():
 
 
 def profile_case(args):
-    """Small deterministic run for ncu captures (same kernels as the timed leg)."""
-    import numpy as np
+    """Small deterministic run for ncu captures (the timed legs' kernels)."""
     import gpue_b200 as G
     if args.profile.endswith("_3d"):
-        # the 256^3 ground-state workload with the launch shapes the large
-        # leg's autotuner picks on a B200 ((16,16) plan, 2/4/4 lines per CTA),
-        # fixed so that a capture does not depend on timings taken under the
-        # profiler; one step here is one imaginary time step (5 passes)
+        # the headline workload with fixed launch shapes for the z pass (and
+        # the x/y line passes of the FP64 form), so a capture does not depend
+        # on timings taken under the profiler; one step is one imaginary time
+        # step (3 passes complex64, 5 passes complex128)
         prec = G.PREC_FP32 if args.profile == "fp32_3d" else G.PREC_FP64
-        n = LARGE["n"]
-        with G.Solver(G.make_params(3, n, LARGE["box"], wz=LARGE["wz"], g=LARGE["g"],
-                                    gdt=LARGE["gdt"], precision=prec)) as s:
+        with G.Solver(head_params(G, prec)) as s:
             for axis, lines in enumerate((2, 4, 4)):
                 s.set_plan(axis, 16, 0, 0, 16, lines)
             plans = [s.plan(a) for a in range(3)]
-            s.set_wfc(gauss_start(3, n, LARGE["box"], LARGE["seed"]))
+            s.set_wfc(head_state())
             r0 = s.evolve(args.warmup, 0)
             r1 = s.evolve(args.steps, 0, step_offset=args.warmup)
         print(json.dumps({"profile": args.profile, "warmup_launches": r0["kernel_launches"],
                           "launches": r1["kernel_launches"], "device_ms": r1["device_ms"],
                           "plans": plans}))
         return
-    n, box = WORK["n"], WORK["box"]
+    import numpy as np
+    n, box = ROT["n"], ROT["box"]
     dx = box / (n >> 1)
     x = -box + dx * np.arange(n)
     psi0 = (np.exp(-(x[None, :] ** 2 + x[:, None] ** 2) / 8.0) *
             np.exp(1j * phase_field(n, box))).astype(np.complex128)
     prec = G.PREC_FP32 if args.profile == "fp32" else G.PREC_FP64
-    with G.Solver(work_params(G, prec, 0)) as s:
+    with G.Solver(rot_params(G, prec, 0)) as s:
         s.set_wfc(psi0)
         # here a step is 2 time steps (one x/y gauge-order cycle), so that
         # captures can pick single launches out of a short run
@@ -642,12 +723,13 @@ def main():
         return
     import torch
     import gpue_b200 as G
+    peak, peak_src = measured_peak()
     if args.only:
-        if args.only == "large":
-            print(json.dumps({"large": large_leg(G, 0, measured_peak()[0])}), flush=True)
-        else:
-            leg = batch_leg if args.only == "batch" else serve_leg
-            print(json.dumps({args.only: leg(G, 0)}), flush=True)
+        legs = {"batch": lambda: batch_leg(G, 0), "serve": lambda: serve_leg(G, 0),
+                "accuracy": lambda: accuracy_leg(G, 0, peak),
+                "rot2d": lambda: rot2d_leg(G, torch, 0, lambda: None),
+                "small2d": lambda: small2d_leg(G, 0)}
+        print(json.dumps({args.only: legs[args.only]()}), flush=True)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -665,89 +747,92 @@ def main():
         if dist is not None:
             dist.barrier()
 
-    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    psi0 = initial_state(G, dev)
-    pts = WORK["n"] ** 2
+    psi0 = head_state()
+    pts = HEAD["n"] ** 3
     res = {}
     plans = {}
     for name, prec in (("fp64", G.PREC_FP64), ("fp32", G.PREC_FP32)):
-        with G.Solver(work_params(G, prec, dev)) as s:
+        with G.Solver(head_params(G, prec, dev)) as s:
             plans[name] = [(p["ra"], p["rb"], p["threads_per_line"], p["lines_per_cta"])
                            for p in s.autotune()]  # later solvers of this shape reuse it
             s.set_wfc(psi0)
             sampler = ClockSampler(dev) if name == "fp32" else None
-            ms, launches, clocks = timed_steps(G, torch, s, args.steps, args.warmup, dev, flush,
-                                               barrier, sampler)
-            steady = None
-            if not args.quick:
-                sms, sl = steady_state(G, s, WORK["total_steps"])
-                steady = {"value": pts * WORK["total_steps"] / (sms * 1e-3), "ms": sms,
-                          "steps": WORK["total_steps"], "launches": sl}
+            ms, launches, clocks = timed_steps(G, torch, s, args.steps, args.warmup, dev,
+                                               barrier, 0, sampler=sampler)
+            E = s.energy()
         ms = replicas.max_over_ranks(ms, dist, dev)
-        res[name] = dict(ms=ms, launches=launches, clocks=clocks, steady=steady)
+        res[name] = dict(ms=ms, launches=launches, clocks=clocks, E=E)
 
     tsteps = args.steps * STEPS_PER_BENCH_STEP
     v32 = world * pts * tsteps / (res["fp32"]["ms"] * 1e-3)
     v64 = world * pts * tsteps / (res["fp64"]["ms"] * 1e-3)
     # legs every rank takes part in (same collectives, same order)
-    e2e = None if args.quick else e2e_leg(G, torch, psi0, dev, dist=dist)
+    e2e = e2e_leg(G, torch, psi0, dev, dist=dist)
     batched = None if args.quick else batch_leg(G, dev, dist=dist)
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
         return
 
-    peak, peak_src = measured_peak()
-    # algorithmic bytes: P = 4 full-field read+write passes per time step for
-    # 2D with the gauge, complex64 (8 B): 2*4*8 = 64 B per grid point and step
-    alg_bytes_per_step = 2 * 4 * 8 * pts
+    # roofline of the dominant kernel, the XY-plane pass: one launch reads and
+    # writes the complex64 field once (2 * 8 bytes per point); its duration is
+    # taken as the step time over the 3 pass launches per step
     per_time_step_s = res["fp32"]["ms"] * 1e-3 / tsteps
-    achieved = alg_bytes_per_step / per_time_step_s / 1e9
+    pass_s = per_time_step_s / PASSES["fp32"]
+    achieved = 2 * 8 * pts / pass_s / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get("cfg2_fp32_pass_bytes_per_launch")
+            traffic = json.load(open(tpath)).get("head_fp32_plane_pass_bytes_per_launch")
         except Exception:
             traffic = None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
-                "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)" if peak_src ==
-                "measured" else "fallback 6.65 TB/s",
-                "note": "achieved = 16 MiB algorithmic bytes per pass launch (read+write of "
-                        "the complex64 field) / mean pass duration (4 passes per time step)"}
+                "peak_source": (peak_src + " (MEASURED_PEAKS.json hbm_gbs)")
+                if peak_src == "measured" else "fallback 6.65 TB/s",
+                "alg_frac_80B": 80 * pts / per_time_step_s / 1e9 / peak,
+                "note": "achieved = 256 MiB algorithmic bytes per pass launch (read+write of "
+                        "the complex64 field) / mean pass duration (the bench step time over "
+                        "its 3 x 100 pass launches, CUDA events on the library's stream); "
+                        "alg_frac_80B counts 80 B per point and step (the five-pass line "
+                        "schedule) against the same peak; traffic is dram read+write bytes "
+                        "per launch of the plane pass from an ncu capture "
+                        "(profiles/traffic.json), not measured in this run"}
 
-    # rank 0 alone; the CPU baseline, serving and the 3D leg only at N = 1
+    # rank 0 alone; the CPU baseline and the extra legs only at N = 1
     cpu = None
     if not args.no_cpu_baseline and world == 1:
         cpu = cpu_oracle_rate(psi0)
-    acc = accuracy_leg(G, psi0, dev)
-    served = None if args.quick or world > 1 else serve_leg(G, dev)
-    large = None if args.quick or world > 1 else large_leg(G, dev, peak)
+    extra = {}
+    if not args.quick and world == 1:
+        extra["accuracy_3d"] = accuracy_leg(G, dev, peak)
+        extra["rotating_2d"] = rot2d_leg(G, torch, dev, barrier)
+        extra["small_2d_fp64"] = small2d_leg(G, dev)
+        extra["serving"] = serve_leg(G, dev)
     line = {
         "metric": METRIC, "value": v32, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": res["fp32"]["ms"] / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded; FP64 imaginary-time relaxed state x smoothed random phase)",
-        "config": {"workload": WORKLOAD_NAME, "grid": WORK["n"], "form": "fused complex64, "
-                   "FP64 operator phases rounded, FP64 reductions",
-                   "step": "one gpue_evolve call of %d split-operator time steps (GPUE's "
-                           "printSteps segment)" % STEPS_PER_BENCH_STEP,
-                   "l2": "flushed before every timed step (256 MiB write); the 8 MiB field "
-                         "stays L2-resident within a step, as in a 20000-step run",
+        "data": "synthetic (seeded Gaussian start, normalised)",
+        "config": {"workload": WORKLOAD_NAME, "grid": HEAD["n"], "form": "fused complex64, "
+                   "FP64-formed operator phases rounded once, FP64 reductions",
+                   "step": "one gpue_evolve call of %d imaginary time steps"
+                           % STEPS_PER_BENCH_STEP,
+                   "l2": "inputs larger than L2: the 128 MiB complex64 field (256 MiB "
+                         "complex128) exceeds the 126 MB L2, no flush",
                    "plans": plans,
                    "parallelism": "replicas" if world > 1 else "single"},
         "plain_fp64": {"value": v64, "ms_per_step": res["fp64"]["ms"] / args.steps,
-                       "fused_fp32_over_plain_fp64": v32 / v64},
-        "steady_state": {"fp32": res["fp32"]["steady"], "fp64": res["fp64"]["steady"],
-                         "note": "one gpue_evolve call of 20000 steps (the configuration's "
-                                 "length), graph-replayed, no L2 flush"},
-        "accuracy": acc,
-        "batched_sweep": batched, "serving": served, "large_3d": large,
+                       "fused_fp32_over_plain_fp64": v32 / v64,
+                       "E_after_timed_steps": res["fp64"]["E"]},
+        "E_fp32_after_timed_steps": res["fp32"]["E"],
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+        "batched_sweep": batched,
         "clocks": res["fp32"]["clocks"],
         "gpu_launches": res["fp32"]["launches"],
     }
+    line.update(extra)
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
