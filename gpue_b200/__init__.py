@@ -28,7 +28,7 @@ GAUGE_ROTATION, GAUGE_CONSTANT = 0, 1
 
 STATUS = {0: "GPUE_OK", 1: "GPUE_ERR_INVALID_ARG", 2: "GPUE_ERR_UNSUPPORTED",
           3: "GPUE_ERR_CUDA", 4: "GPUE_ERR_OUT_OF_MEMORY", 5: "GPUE_ERR_AST",
-          6: "GPUE_ERR_STATE", 7: "GPUE_ERR_TIMEOUT"}
+          6: "GPUE_ERR_STATE", 7: "GPUE_ERR_TIMEOUT", 8: "GPUE_ERR_CANCELLED"}
 
 
 class GpueError(RuntimeError):
@@ -128,7 +128,8 @@ class ServerOpts(C.Structure):
 
 class Request(C.Structure):
     _fields_ = [("params", Params), ("gstate", C.c_int32), ("max_steps", C.c_int32),
-                ("psi0", C.c_void_p), ("psi_out", C.c_void_p), ("tag", C.c_int64)]
+                ("psi0", C.c_void_p), ("psi_out", C.c_void_p), ("tag", C.c_int64),
+                ("deadline_s", C.c_double)]
 
 
 class ServerResult(C.Structure):
@@ -147,7 +148,8 @@ class ServerStats(C.Structure):
                 ("bytes_budget", C.c_int64), ("ticks", C.c_int64),
                 ("kernel_launches", C.c_int64), ("point_steps", C.c_double),
                 ("busy_s", C.c_double), ("admit_s", C.c_double), ("issue_s", C.c_double),
-                ("finish_s", C.c_double)]
+                ("finish_s", C.c_double), ("admitted_in_tick", C.c_int64),
+                ("timed_out", C.c_int64), ("cancelled", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -215,10 +217,11 @@ def lib():
         L.gpue_server_poll.argtypes = [vp, C.POINTER(ServerResult), i32, C.POINTER(i32),
                                        C.c_double]
         L.gpue_server_get_stats.argtypes = [vp, C.POINTER(ServerStats)]
+        L.gpue_server_cancel.argtypes = [vp, C.c_int64]
         L.gpue_server_clock.argtypes = [vp]
         L.gpue_server_clock.restype = C.c_double
         for name in ("gpue_server_create", "gpue_server_destroy", "gpue_server_submit",
-                     "gpue_server_poll", "gpue_server_get_stats"):
+                     "gpue_server_poll", "gpue_server_get_stats", "gpue_server_cancel"):
             getattr(L, name).restype = C.c_int
         for name in ("gpue_default_params", "gpue_ctx_create", "gpue_ctx_destroy",
                      "gpue_set_operators", "gpue_set_wfc", "gpue_get_wfc", "gpue_evolve",
@@ -556,7 +559,9 @@ class Server:
     def __exit__(self, *a):
         self.close()
 
-    def submit(self, params, gstate, max_steps, psi0, tag, want_psi=True):
+    def submit(self, params, gstate, max_steps, psi0, tag, want_psi=True, deadline=0.0):
+        """Queues a solve; deadline (seconds after submission, 0 for none)
+        makes it fail with GPUE_ERR_TIMEOUT when it has not finished by then."""
         a = np.ascontiguousarray(psi0, dtype=np.complex128)
         out = np.empty_like(a) if want_psi else None
         q = Request()
@@ -566,11 +571,19 @@ class Server:
         q.psi0 = a.ctypes.data
         q.psi_out = out.ctypes.data if out is not None else None
         q.tag = tag
+        q.deadline_s = float(deadline)
         self._live[tag] = (a, out)
         st = lib().gpue_server_submit(self._h, C.byref(q))
         if st != 0:
             del self._live[tag]
             raise GpueError(st, lib().gpue_server_last_error(self._h).decode())
+
+    def cancel(self, tag):
+        """Cancels the queued or resident requests with this tag (their
+        results come back with GPUE_ERR_CANCELLED)."""
+        st = lib().gpue_server_cancel(self._h, C.c_int64(tag))
+        if st != 0:
+            raise GpueError(st, "no queued or resident request with tag %d" % tag)
 
     def poll(self, timeout=0.0, cap=256):
         """Finished results as dicts (with "psi" when the output was kept)."""

@@ -10,6 +10,11 @@
 // reached max_steps leave after the tick: their state is written to the
 // caller's buffer, their context freed and their result queued for polling.
 //
+// Deadlines and cancellation are host-side: a request whose deadline has
+// passed, or whose tag was cancelled, leaves the queue at once, or leaves the
+// resident set after the tick in flight with its state at that tick; nothing
+// waits on the device for it.
+//
 // A solve's step index advances by check_steps per tick from 0, so every
 // solve sees evolve()'s step numbering (gauge order i % 2, renormalisation
 // after each imaginary-time step) whatever tick it was admitted in, and its
@@ -20,6 +25,7 @@
 #include <condition_variable>
 #include <deque>
 #include <mutex>
+#include <set>
 #include <thread>
 
 #include "batch_internal.h"
@@ -142,6 +148,8 @@ struct gpue_server {
     std::condition_variable cv_work, cv_done;
     std::deque<Pending> queue;             // guarded by mu
     std::deque<gpue_server_result> done;   // guarded by mu
+    std::set<int64_t> cancel;              // guarded by mu: tags of resident solves to drop
+    std::multiset<int64_t> resident_tags;  // guarded by mu: admitted (or being admitted)
     gpue_server_stats st{};                // guarded by mu
     bool stop = false;                     // guarded by mu
     bool broken = false;                   // guarded by mu
@@ -176,6 +184,27 @@ gpue_server_result make_result(const gpue_request& q, gpue_status status, double
     r.t_admit = t_admit;
     r.t_done = t_done;
     return r;
+}
+
+bool expired(const gpue_request& q, double t_submit, double now) {
+    return q.deadline_s > 0 && now - t_submit > q.deadline_s;
+}
+
+// Drops queued requests whose deadline has passed (worker, before admission).
+void drop_expired(gpue_server* S) {
+    std::lock_guard<std::mutex> lk(S->mu);
+    const double now = now_s(S);
+    for (auto it = S->queue.begin(); it != S->queue.end();) {
+        if (expired(it->req, it->t_submit, now)) {
+            S->done.push_back(make_result(it->req, GPUE_ERR_TIMEOUT, it->t_submit, now, now));
+            S->st.failed++;
+            S->st.timed_out++;
+            it = S->queue.erase(it);
+        } else {
+            ++it;
+        }
+    }
+    S->cv_done.notify_all();
 }
 
 // Context of an admitted request, ready for its first tick.  With tune
@@ -226,6 +255,7 @@ void admit(gpue_server* S, bool tune) {
             if (!fits && !(S->active.empty() && (int64_t)est > S->st.bytes_budget)) return;
             p = S->queue.front();
             S->queue.pop_front();
+            if (fits) S->resident_tags.insert(p.req.tag);
             if (!fits) {
                 // larger than the whole budget: it can never be admitted
                 S->done.push_back(make_result(p.req, GPUE_ERR_OUT_OF_MEMORY, p.t_submit,
@@ -241,6 +271,8 @@ void admit(gpue_server* S, bool tune) {
         std::lock_guard<std::mutex> lk(S->mu);
         S->st.bytes_resident -= (int64_t)est;
         if (st) {
+            auto it = S->resident_tags.find(p.req.tag);
+            if (it != S->resident_tags.end()) S->resident_tags.erase(it);
             if (s.c) gpue_ctx_destroy(s.c);
             S->done.push_back(make_result(p.req, st, p.t_submit, s.t_admit, now_s(S)));
             S->st.failed++;
@@ -250,6 +282,7 @@ void admit(gpue_server* S, bool tune) {
         S->st.bytes_resident += (int64_t)s.bytes;
         if (S->st.bytes_resident > S->st.bytes_peak) S->st.bytes_peak = S->st.bytes_resident;
         S->st.admitted++;
+        if (!tune) S->st.admitted_in_tick++;
         S->st.active++;
         s.serial = S->next_serial++;
         S->active.push_back(s);
@@ -375,8 +408,11 @@ gpue_status issue_run(gpue_server* S, int gstate, Run& R, long& launches, std::s
     return GPUE_OK;
 }
 
-// Finishes a solve: final scaling, copy-out, result, context freed.
-void finish(gpue_server* S, Solve& s, const BatchOut& bo, bool stopped) {
+// Finishes a solve: final scaling, copy-out, result, context freed.  `why`
+// is GPUE_OK for a solve that ran to its end, or the timeout / cancellation
+// status of one that leaves early (its state still goes to psi_out).
+void finish(gpue_server* S, Solve& s, const BatchOut& bo, bool stopped,
+            gpue_status why = GPUE_OK) {
     gpue_ctx* c = s.c;
     gpue_status st = GPUE_OK;
     if (s.req.gstate == 0) c->pending_scale = true;
@@ -384,7 +420,7 @@ void finish(gpue_server* S, Solve& s, const BatchOut& bo, bool stopped) {
     if (!st && s.guard) st = scale_state(c, c->prec, kGuard);
     if (!st && s.req.psi_out) st = gpue_get_wfc(c, s.req.psi_out, GPUE_MEM_HOST, GPUE_C128);
     if (!st && cudaStreamSynchronize(c->stream) != cudaSuccess) st = GPUE_ERR_CUDA;
-    gpue_server_result r = make_result(s.req, st, s.t_submit, s.t_admit, now_s(S));
+    gpue_server_result r = make_result(s.req, st ? st : why, s.t_submit, s.t_admit, now_s(S));
     r.steps_done = stopped ? bo.steps : s.steps;
     r.early_stop = stopped ? 1 : 0;
     r.energy = bo.checks > 0 ? bo.energy : NAN;
@@ -394,6 +430,10 @@ void finish(gpue_server* S, Solve& s, const BatchOut& bo, bool stopped) {
         std::lock_guard<std::mutex> lk(S->mu);
         S->st.bytes_resident -= (int64_t)s.bytes;
         S->st.active--;
+        if (r.status == GPUE_ERR_TIMEOUT) S->st.timed_out++;
+        if (r.status == GPUE_ERR_CANCELLED) S->st.cancelled++;
+        auto it = S->resident_tags.find(s.req.tag);
+        if (it != S->resident_tags.end()) S->resident_tags.erase(it);
     }
     push_result(S, r);
 }
@@ -436,6 +476,12 @@ gpue_status tick_complete(gpue_server* S, long launches, std::string& err) {
     }
     std::vector<char> leave(S->active.size(), 0);
     const auto tf = std::chrono::steady_clock::now();
+    std::set<int64_t> cancel;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        cancel.swap(S->cancel);
+    }
+    const double now = now_s(S);
     for (int g = 0; g < 2; ++g) {
         Run& R = S->run[g];
         if (!R.issued) continue;
@@ -445,16 +491,28 @@ gpue_status tick_complete(gpue_server* S, long launches, std::string& err) {
             s.steps += S->o.check_steps;
             pts += (double)s.c->N * S->o.check_steps;
             const bool stopped = g == 0 && bo.active == 0;
-            if (stopped || s.steps >= s.req.max_steps) {
-                finish(S, s, bo, stopped);
+            gpue_status why = GPUE_OK;
+            if (!stopped && s.steps < s.req.max_steps) {
+                if (cancel.count(s.req.tag)) why = GPUE_ERR_CANCELLED;
+                else if (expired(s.req, s.t_submit, now)) why = GPUE_ERR_TIMEOUT;
+            }
+            if (stopped || s.steps >= s.req.max_steps || why != GPUE_OK) {
+                finish(S, s, bo, stopped, why);
                 leave[R.members[k]] = 1;
                 R.drop_graph();  // its arguments name the context just freed
             }
         }
     }
+    // cancellations of solves admitted during this tick apply after their first
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        for (size_t i = 0; i < S->active.size(); ++i)
+            if ((i >= leave.size() || !leave[i]) && cancel.count(S->active[i].req.tag))
+                S->cancel.insert(S->active[i].req.tag);
+    }
     std::vector<Solve> keep;
     for (size_t i = 0; i < S->active.size(); ++i)
-        if (!leave[i]) keep.push_back(S->active[i]);
+        if (i >= leave.size() || !leave[i]) keep.push_back(S->active[i]);
     S->active.swap(keep);
     const double finish_s =
         std::chrono::duration<double>(std::chrono::steady_clock::now() - tf).count();
@@ -485,13 +543,25 @@ void worker_main(gpue_server* S) {
             std::lock_guard<std::mutex> lk(S->mu);
             S->st.admit_s += dt;
         };
+        drop_expired(S);
         timed_admit(true);
         if (S->active.empty()) continue;
         std::string err;
         long launches = 0;
         gpue_status st = tick_issue(S, launches, err);
-        // requests that arrived meanwhile are set up while the device works
-        if (!st) timed_admit(false);
+        // requests that arrive while the device runs the tick are set up
+        // meanwhile (they join the next tick)
+        while (!st) {
+            timed_admit(false);
+            bool busy = false;
+            for (Run& R : S->run)
+                if (R.issued && cudaStreamQuery(R.stream) == cudaErrorNotReady) busy = true;
+            if (!busy) break;
+            std::unique_lock<std::mutex> lk(S->mu);
+            S->cv_work.wait_for(lk, std::chrono::microseconds(200),
+                                [&] { return S->stop || !S->queue.empty(); });
+            if (S->stop) break;
+        }
         if (!st) st = tick_complete(S, launches, err);
         if (st) {
             // the device state of every resident solve is now unknown; let
@@ -505,6 +575,8 @@ void worker_main(gpue_server* S) {
             std::lock_guard<std::mutex> lk(S->mu);
             S->broken = true;
             S->err = err;
+            S->resident_tags.clear();
+            S->cancel.clear();
             S->st.bytes_resident = 0;
             S->st.active = 0;
             while (!S->queue.empty()) {
@@ -602,6 +674,31 @@ gpue_status gpue_server_submit(gpue_server* S, const gpue_request* q) {
     S->st.submitted++;
     S->cv_work.notify_all();
     return GPUE_OK;
+}
+
+gpue_status gpue_server_cancel(gpue_server* S, int64_t tag) {
+    if (!S) return GPUE_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(S->mu);
+    bool found = false;
+    const double now = now_s(S);
+    for (auto it = S->queue.begin(); it != S->queue.end();) {
+        if (it->req.tag == tag) {
+            S->done.push_back(make_result(it->req, GPUE_ERR_CANCELLED, it->t_submit, now, now));
+            S->st.failed++;
+            S->st.cancelled++;
+            it = S->queue.erase(it);
+            found = true;
+        } else {
+            ++it;
+        }
+    }
+    // resident (or being admitted): the worker drops it after the tick in flight
+    if (S->resident_tags.count(tag)) {
+        S->cancel.insert(tag);
+        found = true;
+    }
+    if (found) S->cv_done.notify_all();
+    return found ? GPUE_OK : GPUE_ERR_INVALID_ARG;
 }
 
 gpue_status gpue_server_poll(gpue_server* S, gpue_server_result* out, int32_t cap, int32_t* n,

@@ -43,7 +43,7 @@
 extern "C" {
 #endif
 
-#define GPUE_B200_ABI_VERSION 1
+#define GPUE_B200_ABI_VERSION 2
 
 typedef enum gpue_status {
     GPUE_OK = 0,
@@ -53,7 +53,9 @@ typedef enum gpue_status {
     GPUE_ERR_OUT_OF_MEMORY = 4, /* device allocation failed or budget exceeded */
     GPUE_ERR_AST = 5,           /* equation string did not parse */
     GPUE_ERR_STATE = 6,         /* call out of order (e.g. no wavefunction set) */
-    GPUE_ERR_TIMEOUT = 7        /* a bounded device wait gave up */
+    GPUE_ERR_TIMEOUT = 7,       /* a bounded device wait gave up, or a served request's
+                                   deadline passed */
+    GPUE_ERR_CANCELLED = 8      /* a served request was cancelled (gpue_server_cancel) */
 } gpue_status;
 
 enum { GPUE_PREC_FP64 = 0, GPUE_PREC_FP32 = 1 };
@@ -434,6 +436,10 @@ typedef struct gpue_request {
     const void* psi0;    /* host complex128, read when the solve is admitted */
     void* psi_out;       /* host complex128, written when it completes; may be NULL */
     int64_t tag;         /* returned with the result */
+    double deadline_s;   /* 0: none; else the request fails with GPUE_ERR_TIMEOUT once this
+                            many seconds have passed since its submission (checked while it
+                            waits and after every tick; a resident solve's state at that
+                            tick is written to psi_out) */
 } gpue_request;
 
 typedef struct gpue_server_result {
@@ -456,6 +462,8 @@ typedef struct gpue_server_stats {
     double admit_s;      /* worker's host time admitting solves (context set-up) */
     double issue_s;      /* worker's host time planning and enqueuing ticks */
     double finish_s;     /* worker's host time returning finished solves */
+    int64_t admitted_in_tick;  /* solves admitted while a tick ran on the device */
+    int64_t timed_out, cancelled;
 } gpue_server_stats;
 
 gpue_status gpue_server_create(const gpue_server_opts* opts, gpue_server** out);
@@ -465,6 +473,13 @@ const char* gpue_server_last_error(const gpue_server* server);
 /* Queues a request (thread-safe); psi0 and psi_out must stay valid until its
  * result is polled. */
 gpue_status gpue_server_submit(gpue_server* server, const gpue_request* req);
+/* Cancels every queued or resident request with this tag: a queued one
+ * leaves at once, a resident one after the tick in flight (its state at that
+ * tick is written to psi_out); their results carry GPUE_ERR_CANCELLED.
+ * GPUE_ERR_INVALID_ARG when no queued or resident request has the tag.
+ * Replaces GPUE's only way to end a run early, the process exit
+ * (src/split_op.cu:40-53). */
+gpue_status gpue_server_cancel(gpue_server* server, int64_t tag);
 /* Moves up to cap finished results into out (*n of them), waiting up to
  * timeout_s seconds when none is ready. */
 gpue_status gpue_server_poll(gpue_server* server, gpue_server_result* out, int32_t cap,

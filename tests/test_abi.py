@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_defaults():
     import gpue_b200 as G
-    assert G.lib().gpue_abi_version() == 1
+    assert G.lib().gpue_abi_version() == 2
     p = G.default_params()
     # parseArgs defaults (src/parser.cu:14-67)
     assert (p.xDim, p.yDim, p.dimnum) == (256, 256, 2)
