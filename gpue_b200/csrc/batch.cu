@@ -61,6 +61,24 @@ std::string pass_signature(const gpue_ctx* c, int prec, const std::vector<LPass>
     return s;
 }
 
+// Lines per tile of a persistent-kernel tile body, and whether the solve's
+// every axis has a body that tiles it.
+int mega_lines(int kind) { return kMegaThreads / mega_threads_per_line(kind); }
+
+bool mega_eligible(const gpue_ctx* c, int prec) {
+    const char* env = std::getenv("GPUE_BATCH_MEGA");
+    if (env && env[0] == '0') return false;
+    if (c->ext || c->time_dep) return false;
+    for (int a = 0; a < c->dim; ++a) {
+        const int kind = mega_kind(kprec(prec), c->ax[a].n, a);
+        if (kind < 0 || mega_plan_ls(kprec(prec), kind) < 0) return false;
+        const int C = mega_lines(kind);
+        const long nlines = c->N / c->ax[a].n;
+        if (nlines % C || (a > 0 && c->ax[0].n % C)) return false;
+    }
+    return true;
+}
+
 void group_solves(BatchRun& r, int probe) {
     r.groups.clear();
     std::map<std::string, int> by_sig;
@@ -77,6 +95,7 @@ void group_solves(BatchRun& r, int probe) {
             BGroup g;
             g.prec = c->prec;
             g.guard = r.guard[i];
+            g.mega = mega_eligible(c, c->prec);
             r.groups.push_back(g);
         }
         r.groups[it->second].members.push_back((int)i);
@@ -99,21 +118,138 @@ gpue_status set_batch_smem(const void* fn, size_t smem, std::string& err) {
 
 }  // namespace
 
+// One k_batch_mega launch for the steps [s0, s1) of every persistent-kernel
+// solve of precision `prec` (after a clear of its counters), appended to ops.
+gpue_status plan_mega(const BatchRun& r, int prec, int s0, int s1, ArgSink& sink,
+                      std::vector<LaunchOp>& ops, long& launches, std::string& err) {
+    std::vector<int> solves;
+    for (const BGroup& g : r.groups)
+        if (g.mega && g.prec == prec)
+            for (int m : g.members) solves.push_back(m);
+    if (solves.empty()) return GPUE_OK;
+    const int ns = (int)solves.size();
+    std::vector<std::vector<LPass>> lists(ns);
+    size_t rounds = 0;
+    for (int k = 0; k < ns; ++k) {
+        const int m = solves[k];
+        lists[k] = solve_passes(r.ctx[m], r.offset[m] + s0, r.offset[m] + s1, r.gstate,
+                                r.guard[m], r.scale_step0);
+        rounds = std::max(rounds, lists[k].size());
+    }
+    // pass instances, round-major, cut into items of about 32K points;
+    // argument blocks stored once per content
+    std::vector<MegaPass> inst;
+    std::vector<int> item_pass;
+    std::vector<PassArgs> args;
+    std::map<std::string, int> arg_index;
+    std::vector<int> last(ns, -1);
+    long start = 0;
+    size_t smem = 2 * (kMegaThreads / 32) * sizeof(double);
+    for (size_t rd = 0; rd < rounds; ++rd) {
+        for (int k = 0; k < ns; ++k) {
+            if (rd >= lists[k].size()) continue;
+            gpue_ctx* c = r.ctx[solves[k]];
+            const LPass& lp = lists[k][rd];
+            PassArgs a;
+            gpue_status st = make_pass_args(c, prec, lp, r.gstate, a);
+            if (st) {
+                err = c->err;
+                return st;
+            }
+            const int n_ax = c->ax[lp.axis].n;
+            const int kind = mega_kind(kprec(prec), n_ax, lp.axis);
+            const int C = mega_lines(kind);
+            a.ntiles = (c->N / n_ax) / C;
+            smem = std::max(smem, (size_t)C * mega_plan_ls(kprec(prec), kind) * elem_size(prec));
+            const std::string key(reinterpret_cast<const char*>(&a), sizeof a);
+            auto it = arg_index.find(key);
+            if (it == arg_index.end()) {
+                it = arg_index.emplace(key, (int)args.size()).first;
+                args.push_back(a);
+            }
+            MegaPass p;
+            p.start = start;
+            p.ntiles = (int)a.ntiles;
+            p.chunk = std::max(1, (int)(32768 / ((long)C * n_ax)));
+            p.nitems = (p.ntiles + p.chunk - 1) / p.chunk;
+            p.dep = last[k];
+            p.kind = kind;
+            p.args = it->second;
+            last[k] = (int)inst.size();
+            for (int i = 0; i < p.nitems; ++i) item_pass.push_back((int)inst.size());
+            inst.push_back(p);
+            start += p.nitems;
+        }
+    }
+    // counters: the ticket (8 bytes) and one completion count per instance
+    std::vector<int> zeros(2 + inst.size(), 0);
+    const void *dinst, *ditems, *dargs, *dctr;
+    gpue_status st = sink.put(inst.data(), inst.size() * sizeof(MegaPass), &dinst, err);
+    if (!st) st = sink.put(item_pass.data(), item_pass.size() * sizeof(int), &ditems, err);
+    if (!st) st = sink.put(args.data(), args.size() * sizeof(PassArgs), &dargs, err);
+    if (!st) st = sink.put(zeros.data(), zeros.size() * sizeof(int), &dctr, err);
+    if (st) return st;
+    void* fn = mega_kernel(kprec(prec));
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) {
+            err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
+            return GPUE_ERR_CUDA;
+        }
+    }
+    int per_sm = 0;
+    gpue_ctx* c0 = r.ctx[solves[0]];
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kMegaThreads, smem) !=
+            cudaSuccess || per_sm < 1) {
+        err = "no resident launch shape for the persistent batched kernel";
+        return GPUE_ERR_CUDA;
+    }
+    const long grid = std::min<long>((long)per_sm * c0->sms, start);
+    MegaArgs ma;
+    ma.passes = static_cast<const MegaPass*>(dinst);
+    ma.item_pass = static_cast<const int*>(ditems);
+    ma.npass = (int)inst.size();
+    ma.total = start;
+    ma.args = static_cast<const PassArgs*>(dargs);
+    ma.ticket = reinterpret_cast<unsigned long long*>(const_cast<void*>(dctr));
+    ma.done = reinterpret_cast<int*>(const_cast<void*>(dctr)) + 2;
+    ma.err = c0->dflags + 3;
+    const size_t ctr_bytes = zeros.size() * sizeof(int);
+    void* ctr = const_cast<void*>(dctr);
+    ops.push_back([=](cudaStream_t s) {
+        cudaMemsetAsync(ctr, 0, ctr_bytes, s);
+        void* params[] = {const_cast<MegaArgs*>(&ma)};
+        cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(kMegaThreads), params, smem, s);
+    });
+    launches++;
+    return GPUE_OK;
+}
+
 gpue_status plan_segment(const BatchRun& r, int s0, int s1, bool check, ArgSink& sink,
                          SegPlan& sp, std::string& err) {
     sp.lanes.assign(r.groups.size(), {});
+    sp.main_ops.clear();
     sp.check = check;
     sp.launches = 0;
+    for (int prec : {GPUE_PREC_FP64, GPUE_PREC_FP32}) {
+        gpue_status st = plan_mega(r, prec, s0, s1, sink, sp.main_ops, sp.launches, err);
+        if (st) return st;
+    }
     for (size_t gi = 0; gi < r.groups.size(); ++gi) {
         const BGroup& g = r.groups[gi];
+        // persistent-kernel groups only add their energy passes, after it
+        if (g.mega && !check) continue;
+        std::vector<LaunchOp>& out_ops = g.mega ? sp.main_ops : sp.lanes[gi];
         const int n = (int)g.members.size();
         gpue_ctx* c0 = r.ctx[g.members[0]];
         std::vector<std::vector<LPass>> lists(n);
         for (int k = 0; k < n; ++k) {
             const int m = g.members[k];
             gpue_ctx* c = r.ctx[m];
-            lists[k] = solve_passes(c, r.offset[m] + s0, r.offset[m] + s1, r.gstate, r.guard[m],
-                                    r.scale_step0);
+            if (!g.mega)
+                lists[k] = solve_passes(c, r.offset[m] + s0, r.offset[m] + s1, r.gstate,
+                                        r.guard[m], r.scale_step0);
             if (check)
                 for (const LPass& lp : energy_passes(c, r.gstate == 0)) lists[k].push_back(lp);
         }
@@ -149,7 +285,7 @@ gpue_status plan_segment(const BatchRun& r, int s0, int s1, bool check, ArgSink&
             const unsigned threads = (unsigned)lc.threads;
             const size_t smem = lc.smem;
             const bool pdl = j > 0;  // follows a pass kernel on this lane
-            sp.lanes[gi].push_back([=](cudaStream_t s) {
+            out_ops.push_back([=](cudaStream_t s) {
                 launch_kernel(fn, grid, threads, smem, s, pdl,
                               static_cast<const PassArgs*>(dargs),
                               static_cast<const long*>(dprefix), n);
@@ -174,7 +310,7 @@ gpue_status plan_segment(const BatchRun& r, int s0, int s1, bool check, ArgSink&
             const unsigned grid = (unsigned)(n * per);
             const int iper = (int)per;
             const bool f32 = g.prec == GPUE_PREC_FP32;
-            sp.lanes[gi].push_back([=](cudaStream_t s) {
+            out_ops.push_back([=](cudaStream_t s) {
                 const EnergyArgs* e = static_cast<const EnergyArgs*>(dea);
                 const int* const* a = static_cast<const int* const*>(dact);
                 if (f32) k_energy_real_batch<float><<<grid, 256, 0, s>>>(e, a, iper);
@@ -221,12 +357,16 @@ void enqueue_segment(const SegPlan& sp, const BatchRun& r, cudaStream_t main, La
                      const CheckArgs* checks, int* nactive) {
     cudaEventRecord(lanes.fork, main);
     for (size_t gi = 0; gi < sp.lanes.size(); ++gi) {
+        if (sp.lanes[gi].empty()) continue;
         cudaStream_t s = lanes.streams[gi];
         cudaStreamWaitEvent(s, lanes.fork, 0);
         for (const LaunchOp& op : sp.lanes[gi]) op(s);
         cudaEventRecord(lanes.joins[gi], s);
-        cudaStreamWaitEvent(main, lanes.joins[gi], 0);
     }
+    // the persistent launches run on the main stream while the lanes run
+    for (const LaunchOp& op : sp.main_ops) op(main);
+    for (size_t gi = 0; gi < sp.lanes.size(); ++gi)
+        if (!sp.lanes[gi].empty()) cudaStreamWaitEvent(main, lanes.joins[gi], 0);
     if (sp.check)
         k_batch_check<<<1, 256, 0, main>>>(checks, (int)r.ctx.size(), r.every, r.step_base,
                                             r.thr, r.thr_abs, r.gstate == 0 ? 1 : 0, nactive);

@@ -7,8 +7,16 @@
 // between a fork and a join; after the join one block evaluates every solve's
 // energy check (k_batch_check) and clears the active flag of those that
 // stopped, which freezes them: every later kernel skips their tiles.
+//
+// Solves whose every axis has a length the persistent multi-size kernel
+// covers (batch_mega.cuh) take no group launches for their steps: all of them,
+// whatever their sizes, run in one k_batch_mega launch per segment and
+// precision, on the main stream while the other groups' lanes run.  Their
+// energy passes follow on the main stream.  GPUE_BATCH_MEGA=0 keeps every
+// solve on group launches.
 #pragma once
 
+#include "batch_mega.cuh"
 #include "engine_internal.h"
 
 namespace gpue_eng {
@@ -24,6 +32,7 @@ struct ArgSink {
 struct BGroup {
     int prec = 0;
     bool guard = false;
+    bool mega = false;         // its solves run on the persistent multi-size kernel
     std::vector<int> members;  // indices into BatchRun::ctx
 };
 
@@ -44,6 +53,7 @@ using LaunchOp = std::function<void(cudaStream_t)>;
 
 struct SegPlan {
     std::vector<std::vector<LaunchOp>> lanes;  // one list per group
+    std::vector<LaunchOp> main_ops;            // the persistent launches and what follows them
     bool check = false;
     long launches = 0;
 };

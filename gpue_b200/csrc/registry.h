@@ -38,6 +38,14 @@ struct PlaneKernel {
 // nullptr when no plane pass is compiled for (precision, n)
 const PlaneKernel* find_plane_kernel(int prec, int n);
 
+// The persistent multi-size batched kernel (kernels_mega.cu): the tile body
+// ("kind") of a line length and axis, -1 when the length is not covered;
+// threads per line of a kind; the line stride of its plan; the kernel.
+int mega_kind(int prec, int n, int axis);
+int mega_threads_per_line(int kind);
+int mega_plan_ls(int prec, int kind);
+void* mega_kernel(int prec);
+
 // The default plan for a length; nullptr when none is compiled
 const PassKernel* find_pass_kernel(int prec, int n);
 // All plans for a length, default first; returns how many (at most cap)
