@@ -380,8 +380,10 @@ def small2d_leg(G, dev):
 # every 100 steps with the absolute |dE| < 1e-10 stop, fused complex64.
 BATCH = dict(solves=96, sizes=(128, 192, 256, 384, 512), box=10.0, gdt=1e-4, every=100,
              thr=1e-10, seed=4)
-# the sample timed: steps 0..1000 (checks at 0, 100, ..., 1000) of every solve
+# the sample timed both ways: steps 0..1000 (checks at 0, 100, ..., 1000)
 BATCH_STEPS = 1001
+# the run to convergence stops every solve at this many steps at most
+BATCH_CAP = 100000
 
 
 def batch_cases():
@@ -396,11 +398,15 @@ def batch_cases():
     return out
 
 
-def batch_leg(G, dev, steps=BATCH_STEPS, dist=None):
+def batch_leg(G, dev, steps=BATCH_STEPS, dist=None, converge=True):
     """The 96 solves as one gpue_batch against the same solves run one after
-    another through gpue_evolve (same form, same checks).  Under several
-    ranks each GPU takes every world-th solve (no communication) and the
-    rates are all ranks' point-steps over the slowest rank's time."""
+    another through gpue_evolve (same form, same checks): steps 0..1000 both
+    ways, then the batch run on until every solve has converged (|dE| < 1e-10
+    between 100-step checks, capped at BATCH_CAP steps), with the sequential
+    time of that run estimated from each solve's measured per-step time times
+    the steps it ran.  Under several ranks each GPU takes every world-th solve
+    (no communication) and the rates are all ranks' point-steps over the
+    slowest rank's time."""
     world = dist.get_world_size() if dist is not None else 1
     rank = dist.get_rank() if dist is not None else 0
     cs = [batch_cases()[i] for i in replicas.shard(BATCH["solves"], world, rank)]
@@ -412,6 +418,7 @@ def batch_leg(G, dev, steps=BATCH_STEPS, dist=None):
 
     kw = dict(energy_every=BATCH["every"], threshold=BATCH["thr"], threshold_abs=True)
     solvers = [G.Solver(params(c)) for c in cs]
+    conv = None
     try:
         for s, p in zip(solvers, psi0):
             s.set_wfc(p)
@@ -420,31 +427,54 @@ def batch_leg(G, dev, steps=BATCH_STEPS, dist=None):
             for s, p in zip(solvers, psi0):
                 s.set_wfc(p)
             res, st = b.evolve(0, steps, **kw)
+            if converge:
+                for s, p in zip(solvers, psi0):
+                    s.set_wfc(p)
+                cres, cst = b.evolve(0, BATCH_CAP, **kw)
         batched, _, bsecs = replicas.job_rate(st["point_steps"], st["device_ms"] * 1e-3, dist,
                                               dev)
         # sequential: the same solves, one gpue_evolve call each
-        seq_ms, seq_pts = 0.0, 0.0
-        for s, p, c in zip(solvers, psi0, cs):
+        seq_ms, seq_pts, seq_conv_ms = 0.0, 0.0, 0.0
+        for k, (s, p, c) in enumerate(zip(solvers, psi0, cs)):
             s.set_wfc(p)
             s.evolve(2 * BATCH["every"] + 1, 0, **kw)  # graphs of this solve
             s.set_wfc(p)
             r = s.evolve(steps, 0, **kw)
             seq_ms += r["device_ms"]
             seq_pts += c["n"] ** 2 * r["steps_done"]
+            if converge:
+                seq_conv_ms += r["device_ms"] / r["steps_done"] * cres[k]["steps_done"]
     finally:
         for s in solvers:
             s.close()
     sequential, _, ssecs = replicas.job_rate(seq_pts, seq_ms * 1e-3, dist, dev)
-    return {"solves": BATCH["solves"], "ranks": world, "steps": steps, "value": batched,
-            "unit": UNIT, "device_ms": bsecs * 1e3, "kernel_launches": st["kernel_launches"],
-            "graph_launches": st["graph_launches"],
-            "stopped": sum(r["early_stop"] for r in res),
-            "sequential_value": sequential, "sequential_device_ms": ssecs * 1e3,
-            "batched_over_sequential": batched / sequential,
-            "sample": "steps 0..%d of all 96 solves (checks every 100 steps, |dE|<1e-10 "
-                      "absolute stop; none is expected to stop this early), complex64 with "
-                      "FP64 reductions; sequential = the same solves through gpue_evolve one "
-                      "after another (sum of their device times)" % (steps - 1)}
+    out = {"solves": BATCH["solves"], "ranks": world, "steps": steps, "value": batched,
+           "unit": UNIT, "device_ms": bsecs * 1e3, "kernel_launches": st["kernel_launches"],
+           "graph_launches": st["graph_launches"],
+           "stopped": sum(r["early_stop"] for r in res),
+           "sequential_value": sequential, "sequential_device_ms": ssecs * 1e3,
+           "batched_over_sequential": batched / sequential,
+           "sample": "steps 0..%d of all 96 solves (checks every 100 steps, |dE|<1e-10 "
+                     "absolute stop), complex64 with FP64 reductions; sequential = the same "
+                     "solves through gpue_evolve one after another (sum of their device "
+                     "times)" % (steps - 1)}
+    if converge:
+        cval, _, csecs = replicas.job_rate(cst["point_steps"], cst["device_ms"] * 1e-3, dist,
+                                           dev)
+        sval, _, sconv = replicas.job_rate(cst["point_steps"], seq_conv_ms * 1e-3, dist, dev)
+        steps_done = sorted(r["steps_done"] for r in cres)
+        out["to_convergence"] = {
+            "value": cval, "unit": UNIT, "device_ms": csecs * 1e3,
+            "converged": sum(r["early_stop"] for r in cres), "cap_steps": BATCH_CAP,
+            "steps_min": steps_done[0], "steps_median": steps_done[len(steps_done) // 2],
+            "steps_max": steps_done[-1], "kernel_launches": cst["kernel_launches"],
+            "sequential_value_estimated": sval, "sequential_device_ms_estimated": sconv * 1e3,
+            "batched_over_sequential": cval / sval,
+            "note": "every solve from its seeded start until |dE|<1e-10 between 100-step "
+                    "checks (or the cap), converged solves frozen while the rest run on; "
+                    "sequential estimated as each solve's per-step device time through "
+                    "gpue_evolve (measured over steps 0..1000) times the steps it ran here"}
+    return out
 
 
 # -------------------------------------------------------------- serving ---

@@ -136,8 +136,20 @@ gpue_status plan_mega(const BatchRun& r, int prec, int s0, int s1, ArgSink& sink
                                 r.guard[m], r.scale_step0);
         rounds = std::max(rounds, lists[k].size());
     }
-    // pass instances, round-major, cut into items of about 32K points;
-    // argument blocks stored once per content
+    void* fn = mega_kernel(kprec(prec));
+    int per_sm = 0;
+    gpue_ctx* c0 = r.ctx[solves[0]];
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kMegaThreads,
+                                                      48 * 1024) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    // work items of about 32K points, fewer when the solves are too few to
+    // give every resident CTA work (a converged batch's tail)
+    double round_pts = 0;
+    for (int k = 0; k < ns; ++k) round_pts += (double)r.ctx[solves[k]]->N;
+    const long item_pts =
+        std::max(2048L, std::min(32768L, (long)(round_pts / ((double)per_sm * c0->sms))));
+    // pass instances, round-major, cut into items; argument blocks stored once
+    // per content
     std::vector<MegaPass> inst;
     std::vector<int> item_pass;
     std::vector<PassArgs> args;
@@ -170,7 +182,7 @@ gpue_status plan_mega(const BatchRun& r, int prec, int s0, int s1, ArgSink& sink
             MegaPass p;
             p.start = start;
             p.ntiles = (int)a.ntiles;
-            p.chunk = std::max(1, (int)(32768 / ((long)C * n_ax)));
+            p.chunk = std::max(1, (int)(item_pts / ((long)C * n_ax)));
             p.nitems = (p.ntiles + p.chunk - 1) / p.chunk;
             p.dep = last[k];
             p.kind = kind;
@@ -189,7 +201,6 @@ gpue_status plan_mega(const BatchRun& r, int prec, int s0, int s1, ArgSink& sink
     if (!st) st = sink.put(args.data(), args.size() * sizeof(PassArgs), &dargs, err);
     if (!st) st = sink.put(zeros.data(), zeros.size() * sizeof(int), &dctr, err);
     if (st) return st;
-    void* fn = mega_kernel(kprec(prec));
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
@@ -198,8 +209,6 @@ gpue_status plan_mega(const BatchRun& r, int prec, int s0, int s1, ArgSink& sink
             return GPUE_ERR_CUDA;
         }
     }
-    int per_sm = 0;
-    gpue_ctx* c0 = r.ctx[solves[0]];
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kMegaThreads, smem) !=
             cudaSuccess || per_sm < 1) {
         err = "no resident launch shape for the persistent batched kernel";
@@ -368,7 +377,8 @@ void enqueue_segment(const SegPlan& sp, const BatchRun& r, cudaStream_t main, La
     for (size_t gi = 0; gi < sp.lanes.size(); ++gi)
         if (!sp.lanes[gi].empty()) cudaStreamWaitEvent(main, lanes.joins[gi], 0);
     if (sp.check)
-        k_batch_check<<<1, 256, 0, main>>>(checks, (int)r.ctx.size(), r.every, r.step_base,
+        k_batch_check<<<1, 256, 0, main>>>(r.checks ? r.checks : checks, (int)r.ctx.size(),
+                                            r.every, r.step_base,
                                             r.thr, r.thr_abs, r.gstate == 0 ? 1 : 0, nactive);
 }
 
@@ -639,22 +649,28 @@ gpue_status gpue_batch_evolve(gpue_batch* b, int32_t gstate, const gpue_batch_op
         BCK(cudaStreamSynchronize(c->stream));
         pts += (double)c->N;
     }
+    r.checks = b->checks;
+    const std::vector<bool> guard_all = r.guard;
     group_solves(r, 3);
-    // graphs depend on the grouping and on the check parameters
-    std::string gkey = std::to_string(gstate) + ":" + std::to_string(r.every) + ":" +
-                       std::to_string(r.thr_abs) + ":";
-    {
+    // graphs depend on the grouping, the members and the check parameters
+    std::vector<int> ids(n);  // batch index of each solve of r
+    for (int i = 0; i < n; ++i) ids[i] = i;
+    auto make_key = [&](const BatchRun& run, const std::vector<int>& id) {
+        std::string k = std::to_string(gstate) + ":" + std::to_string(run.every) + ":" +
+                        std::to_string(run.thr_abs) + ":";
         char tb[32];
-        std::snprintf(tb, sizeof tb, "%a:", r.thr);
-        gkey += tb;
-        for (const BGroup& g : r.groups) {
-            gkey += "{" + std::to_string(g.guard) + "/" +
-                    pass_signature(r.ctx[g.members[0]], g.prec,
-                                   solve_passes(r.ctx[g.members[0]], 0, 3, gstate, g.guard,
-                                                false)) + "}";
-            for (int m : g.members) gkey += std::to_string(m) + ",";
+        std::snprintf(tb, sizeof tb, "%a:", run.thr);
+        k += tb;
+        for (const BGroup& g : run.groups) {
+            k += "{" + std::to_string(g.guard) + "/" +
+                 pass_signature(run.ctx[g.members[0]], g.prec,
+                                solve_passes(run.ctx[g.members[0]], 0, 3, gstate, g.guard,
+                                             false)) + "}";
+            for (int m : g.members) k += std::to_string(id[m]) + ",";
         }
-    }
+        return k;
+    };
+    std::string gkey = make_key(r, ids);
     const int every = r.every;
     const std::vector<SegSpec> sched =
         batch_schedule(o.max_steps, every, every > 0 ? std::min(every + 1, 256) : 128);
@@ -706,11 +722,60 @@ gpue_status gpue_batch_evolve(gpue_batch* b, int32_t gstate, const gpue_batch_op
             BCK(cudaMemcpyAsync(b->h_nactive + slot, b->nactive, sizeof(int),
                                 cudaMemcpyDeviceToHost, b->stream));
             BCK(cudaEventRecord(b->polled[slot], b->stream));
+            int running = -1;
             if (polls > 0) {
                 BCK(cudaEventSynchronize(b->polled[1 - slot]));
-                if (b->h_nactive[1 - slot] == 0) all_done = true;
+                running = b->h_nactive[1 - slot];
+                if (running == 0) all_done = true;
             }
             polls++;
+            // once half the planned solves have converged, plan the rest alone:
+            // the frozen ones' work items and the coarse items of a full batch
+            // would otherwise dominate the tail
+            if (running > 0 && 2 * running <= (int)r.ctx.size() && e < sched.size()) {
+                BCK(cudaStreamSynchronize(b->stream));
+                k_batch_gather<<<(n + 127) / 128, 128, 0, b->stream>>>(b->checks, n, b->outs);
+                BCK(cudaGetLastError());
+                BCK(cudaMemcpyAsync(b->h_outs, b->outs, n * sizeof(BatchOut),
+                                    cudaMemcpyDeviceToHost, b->stream));
+                BCK(cudaStreamSynchronize(b->stream));
+                BatchRun r2 = r;
+                r2.ctx.clear();
+                r2.offset.clear();
+                r2.guard.clear();
+                std::vector<int> ids2;
+                std::vector<CheckArgs> ca;
+                for (int i = 0; i < n; ++i) {
+                    if (!b->h_outs[i].active) continue;
+                    gpue_ctx* c = b->ctx[i];
+                    r2.ctx.push_back(c);
+                    r2.offset.push_back(0);
+                    r2.guard.push_back(guard_all[i]);
+                    ids2.push_back(i);
+                    CheckArgs x;
+                    x.scal = c->scal;
+                    x.flags = c->dflags;
+                    x.inv_n = 1.0 / (double)c->N;
+                    x.dV = c->dV;
+                    x.slot_ekin = kEkin;
+                    x.slot_ereal = kEreal;
+                    x.slot_eold = kEold;
+                    x.slot_e = kEcheck;
+                    ca.push_back(x);
+                }
+                if (!r2.ctx.empty()) {
+                    const void* dca = nullptr;
+                    gpue_status st =
+                        b->args.put(ca.data(), ca.size() * sizeof(CheckArgs), &dca, b->err);
+                    if (st) return st;
+                    r2.checks = static_cast<const CheckArgs*>(dca);
+                    group_solves(r2, 3);
+                    r = r2;
+                    ids = ids2;
+                    gkey = make_key(r, ids);
+                    polls = 0;
+                }
+            }
         }
         s = e;
     }
@@ -737,7 +802,7 @@ gpue_status gpue_batch_evolve(gpue_batch* b, int32_t gstate, const gpue_batch_op
         if (bo.checks > 0) c->last_energy = bo.energy;
         if (gstate == 0) c->pending_scale = true;
         BCTX(c, apply_pending_scale(c, c->prec));
-        if (r.guard[i]) BCTX(c, scale_state(c, c->prec, kGuard));
+        if (guard_all[i]) BCTX(c, scale_state(c, c->prec, kGuard));
     }
     for (int i = 0; i < n; ++i) BCK(cudaStreamSynchronize(b->ctx[i]->stream));
     if (stats) {

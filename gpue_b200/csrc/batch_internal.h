@@ -44,6 +44,7 @@ struct BatchRun {
     int thr_abs = 0;
     bool scale_step0 = false;     // renormalise (by scal[kScale]) before step 0 too
     std::vector<gpue_ctx*> ctx;   // the solves
+    const CheckArgs* checks = nullptr;  // device, one per solve of ctx (k_batch_check)
     std::vector<int> offset;      // per solve: its step index at segment step 0
     std::vector<bool> guard;      // per solve: real-time norm guard
     std::vector<BGroup> groups;
@@ -79,7 +80,8 @@ struct Lanes {
     void destroy();
 };
 // Enqueues a planned segment on `main`: groups fork onto lanes, join back,
-// then k_batch_check over all solves when the segment has a check.
+// then k_batch_check over all solves (r.checks, else `checks`) when the
+// segment has a check.
 void enqueue_segment(const SegPlan& sp, const BatchRun& r, cudaStream_t main, Lanes& lanes,
                      const CheckArgs* checks, int* nactive);
 
