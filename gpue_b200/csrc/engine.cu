@@ -352,6 +352,64 @@ gpue_status plan_plane(gpue_ctx* c, int prec) {
     return GPUE_OK;
 }
 
+namespace {
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library links only the runtime)
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                 const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                 const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_tiled() {
+    static EncodeTiled fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (EncodeTiled) nullptr;
+        return reinterpret_cast<EncodeTiled>(p);
+    }();
+    return fn;
+}
+
+}  // namespace
+
+gpue_status plan_zpass(gpue_ctx* c, int prec) {
+    ZCfg& zc = c->zpass[prec];
+    zc.k = nullptr;
+    const char* env = std::getenv("GPUE_ZTMA");
+    if (env && env[0] == '0') return GPUE_OK;
+    if (c->dim != 3 || c->ax[0].n % 16 || c->ax[2].n > 256) return GPUE_OK;
+    const ZPassKernel* k = find_zpass_kernel(kprec(prec), c->ax[2].n);
+    EncodeTiled enc = encode_tiled();
+    if (!k || !enc) return GPUE_OK;
+    int max_smem = 0;
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+    if (k->smem > max_smem) return GPUE_OK;
+    CK(cudaFuncSetAttribute(k->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, k->smem));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k->fn, k->threads, k->smem));
+    if (per_sm < 1) return GPUE_OK;
+    // the field as nx x ny x nz elements of 8 bytes (one complex64 each); a
+    // box is 16 x-columns of one y-row over all planes
+    const cuuint64_t dims[3] = {(cuuint64_t)c->ax[0].n, (cuuint64_t)c->ax[1].n,
+                                (cuuint64_t)c->ax[2].n};
+    const cuuint64_t strides[2] = {(cuuint64_t)c->ax[0].n * 8,
+                                   (cuuint64_t)c->ax[0].n * c->ax[1].n * 8};
+    const cuuint32_t box[3] = {16, 1, (cuuint32_t)c->ax[2].n};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    if (enc(&zc.tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, state_of(c, prec), dims, strides, box,
+            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return GPUE_OK;
+    const long tiles = (long)(c->ax[0].n / 16) * c->ax[1].n;
+    zc.blocks = (int)std::min<long>((long)per_sm * c->sms, tiles);
+    zc.k = k;
+    return GPUE_OK;
+}
+
 bool plane_ok(const gpue_ctx* c, int prec) {
     if (!c->plane[prec].k || c->ext) return false;
     return !(c->p.corotating && (axis_gauge_active(c, 0) || axis_gauge_active(c, 1)));
@@ -458,6 +516,25 @@ gpue_status launch_pass(gpue_ctx* c, int prec, const LPass& lp, int gstate, bool
         cfg.attrs = at;
         cfg.numAttrs = pdl ? 2 : 1;
         CK(cudaLaunchKernelEx(&cfg, lp.axis == kPlaneFwd ? pc.k->fwd : pc.k->inv, a));
+        c->launches++;
+        return GPUE_OK;
+    }
+    const ZCfg& zc = c->zpass[prec];
+    if (lp.axis == 2 && zc.k && !c->ext && lp.red == RED_NONE && lp.store &&
+        !lp.from_scratch && !lp.to_scratch && a.in == state_of(c, prec) &&
+        lp.ops == std::vector<int>{OP_FFT_F, OP_KPHASE, OP_FFT_I}) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(zc.blocks);
+        cfg.blockDim = dim3(zc.k->threads);
+        cfg.dynamicSmemBytes = zc.k->smem;
+        cfg.stream = c->stream;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = pdl ? 1 : 0;
+        void* args[] = {const_cast<CUtensorMap*>(&zc.tm), &a};
+        CK(cudaLaunchKernelExC(&cfg, zc.k->fn, args));
         c->launches++;
         return GPUE_OK;
     }
@@ -1136,6 +1213,7 @@ gpue_status gpue_ctx_create(const gpue_params* p, gpue_ctx** out) {
         if (st) return st;
     }
     st = plan_plane(c, c->prec);
+    if (!st) st = plan_zpass(c, c->prec);
     if (st) return st;
     const char* tune = std::getenv("GPUE_AUTOTUNE");
     if (tune && tune[0] == '1') {

@@ -2,6 +2,7 @@
 // server translation units (not part of the public ABI).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -68,6 +69,14 @@ struct PlaneCfg {
 // LPass::axis values of the two plane passes
 enum { kPlaneFwd = 3, kPlaneInv = 4 };
 
+// The TMA z pass of a 3D context (zpass.cuh): the kernel and the tensor map
+// of the context's resident field
+struct ZCfg {
+    const ZPassKernel* k = nullptr;
+    CUtensorMap tm;
+    int blocks = 0;
+};
+
 struct GraphKey {
     int prec, gstate, parity, nsteps, scale_first, energy_last, guard, observables;
     bool operator<(const GraphKey& o) const {
@@ -106,6 +115,7 @@ struct gpue_ctx {
     gpue_eng::Tables tab[2];            // indexed by GPUE_PREC_*
     gpue_eng::LaunchCfg lc[2][3];       // [precision][axis]
     gpue_eng::PlaneCfg plane[2];        // [precision]: XY-plane passes, if any
+    gpue_eng::ZCfg zpass[2];            // [precision]: the TMA z pass, if any
     bool have_wfc = false;
     bool pending_scale = false;  // scal[kScale] must multiply psi
     std::map<gpue_eng::GraphKey, gpue_eng::Segment> graphs;
@@ -217,6 +227,9 @@ void step_passes(gpue_ctx* c, int i, int gstate, bool scale_first, double rexp, 
 // Plans the XY-plane passes of precision prec when the context qualifies
 // (3D, nx = ny with a compiled plane kernel); leaves them off otherwise.
 gpue_status plan_plane(gpue_ctx* c, int prec);
+// Plans the TMA z pass of precision prec when the context qualifies (3D, nx a
+// multiple of 16, nz <= 256 with a compiled kernel).
+gpue_status plan_zpass(gpue_ctx* c, int prec);
 // The plane passes can run this context's steps now (no table or expression
 // fields, no in-plane gauge).
 bool plane_ok(const gpue_ctx* c, int prec);

@@ -1,8 +1,9 @@
-// kernels_plane.cu -- the complex64 XY-plane pass kernels (plane.cuh) for the
-// 3D step, one forward/inverse pair per in-plane length, each with the line
-// length's default radix plan.
+// kernels_plane.cu -- the complex64 XY-plane pass kernels (plane.cuh) and the
+// TMA z pass (zpass.cuh) for the 3D step, per length with the line length's
+// default radix plan.
 #include "registry.h"
 #include "plane.cuh"
+#include "zpass.cuh"
 
 namespace gpue {
 
@@ -21,6 +22,27 @@ static const PlaneKernel kPlanesF32[] = {
     GPUE_PLANE(float, 192, 4, 12, 0, 16),
     GPUE_PLANE(float, 256, 16, 0, 0, 16),
 };
+
+#define GPUE_ZPASS(T, N, RA, RB, RC, P)                                                     \
+    ZPassKernel{N, RA, RB, RC, P, ZShape<T, N, RA, RB, P, RC>::THREADS,                      \
+                (int)ZShape<T, N, RA, RB, P, RC>::SMEM,                                      \
+                (const void*)&k_zpass<T, N, RA, RB, P, RC>}
+
+static const ZPassKernel kZPassF32[] = {
+    GPUE_ZPASS(float, 64, 4, 4, 0, 16),
+    GPUE_ZPASS(float, 96, 4, 6, 0, 8),
+    GPUE_ZPASS(float, 128, 4, 8, 0, 16),
+    GPUE_ZPASS(float, 160, 4, 10, 0, 8),
+    GPUE_ZPASS(float, 192, 4, 12, 0, 16),
+    GPUE_ZPASS(float, 256, 16, 0, 0, 16),
+};
+
+const ZPassKernel* find_zpass_kernel(int prec, int n) {
+    if (prec != PREC_F32) return nullptr;
+    for (const ZPassKernel& k : kZPassF32)
+        if (k.n == n) return &k;
+    return nullptr;
+}
 
 const PlaneKernel* find_plane_kernel(int prec, int n) {
     if (prec != PREC_F32) return nullptr;

@@ -38,6 +38,18 @@ struct PlaneKernel {
 // nullptr when no plane pass is compiled for (precision, n)
 const PlaneKernel* find_plane_kernel(int prec, int n);
 
+// The TMA z pass (zpass.cuh) for 3D fields with nz = n: tiles of 16 x-columns,
+// `threads` threads and `smem` bytes per CTA; its first parameter is the
+// CUtensorMap of the field (passed as void* here to keep cuda.h out).
+struct ZPassKernel {
+    int n;
+    int ra, rb, rc, p;
+    int threads;
+    int smem;
+    const void* fn;
+};
+const ZPassKernel* find_zpass_kernel(int prec, int n);
+
 // The persistent multi-size batched kernel (kernels_mega.cu): the tile body
 // ("kind") of a line length and axis, -1 when the length is not covered;
 // threads per line of a kind; the line stride of its plan; the kernel.

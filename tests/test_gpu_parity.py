@@ -145,3 +145,36 @@ def test_fp32_ground_state_energy_gate(G):
     assert abs(E32 - E64) <= 1e-6 * abs(E64)
     assert abs(E32p - E64) <= 1e-7 * abs(E64)
     assert psi.dtype == np.complex128
+
+
+STRONG = [
+    # the nonlinear angle gN|psi|^2 Dt/2 reaches ~0.3 at the peak, past the
+    # 1/16 where the complex64 form leaves its FP32 Taylor series for the
+    # factor formed in FP64 from the FP64 angle
+    dict(dim=2, n=64, box=6.0, g=2000.0, gdt=1e-3, gsteps=60, seed=31, init="gauss",
+         energy_every=20),
+    dict(dim=2, n=64, box=6.0, g=2000.0, dt=1e-3, esteps=60, seed=32, init="phase",
+         energy_every=20),
+    dict(dim=3, n=32, box=5.0, wz=2.0, g=3000.0, dt=1e-3, esteps=40, seed=33, init="phase",
+         energy_every=20),
+]
+
+
+@pytest.mark.parametrize("k", range(len(STRONG)))
+def test_fp32_large_nonlinear_angles_match_oracle(G, k):
+    c = dict(cases.DEFAULTS)
+    c.update(STRONG[k])
+    psi0 = cases.initial_psi(c)
+    steps, gs = steps_gstate(c)
+    peak = float(np.max(np.abs(psi0) ** 2)) * c["g"] * (c["gdt"] if gs == 0 else c["dt"]) / 2
+    assert peak > 1.0 / 16.0
+    P = oracle_problem(c)
+    ref, _, _ = P.evolve(psi0, steps, gs)
+    Eref = P.energy(ref)
+    psi, E, r = run_product(c, G.PREC_FP32, psi0=psi0)
+    assert abs(E - Eref) <= 1e-5 * abs(Eref)
+    # strong coupling amplifies complex64 round-off into the phase: the
+    # fixture tolerance of the other FP32 parity tests, 5e-4, is kept tighter
+    assert l2(psi, ref, c) <= 1e-4
+    psi64, E64, _ = run_product(c, G.PREC_FP64, psi0=psi0)
+    assert l2(psi64, ref, c) <= 1e-12

@@ -21,20 +21,22 @@ pytestmark = pytest.mark.gpu
 PLANE_LENGTHS = [64, 96, 128, 160, 192, 256]
 
 
-def run(c, steps, gstate, plane, psi0):
+def run(c, steps, gstate, plane, psi0, ztma=True):
     import gpue_b200 as G
-    old = os.environ.get("GPUE_PLANE")
+    old = {k: os.environ.get(k) for k in ("GPUE_PLANE", "GPUE_ZTMA")}
     os.environ["GPUE_PLANE"] = "1" if plane else "0"
+    os.environ["GPUE_ZTMA"] = "1" if ztma else "0"
     try:
         with G.Solver(product_params(c, G.PREC_FP32)) as s:
             s.set_wfc(psi0)
             r = s.evolve(steps, gstate, energy_every=c["energy_every"])
             return s.get_wfc(), s.energy(), r
     finally:
-        if old is None:
-            del os.environ["GPUE_PLANE"]
-        else:
-            os.environ["GPUE_PLANE"] = old
+        for k, v in old.items():
+            if v is None:
+                del os.environ[k]
+            else:
+                os.environ[k] = v
 
 
 @pytest.mark.parametrize("gstate", [0, 1], ids=["imag", "real"])
@@ -58,6 +60,20 @@ def test_plane_schedule_matches_oracle_and_line_schedule(n, gstate):
     assert abs(r["energy"] - en[-1]) <= 1e-5 * abs(en[-1])
     # three passes per step instead of five
     assert r["kernel_launches"] < rl["kernel_launches"]
+
+
+@pytest.mark.parametrize("n", PLANE_LENGTHS)
+def test_tma_z_pass_matches_the_line_z_pass(n):
+    """The TMA-fed z pass moves data differently but runs the same operations
+    as the line pass along z: the two agree to complex64 round-off (the
+    compiler may contract multiply-adds differently in the two kernels)."""
+    c = dict(cases.DEFAULTS, dim=3, n=n, box=8.0, wz=2.5, g=200.0, dt=1e-4, seed=520 + n,
+             init="phase", energy_every=0)
+    psi0 = cases.initial_psi(c)
+    a, Ea, ra = run(c, 4, 1, True, psi0, ztma=True)
+    b, Eb, rb = run(c, 4, 1, True, psi0, ztma=False)
+    assert float(np.sqrt(np.sum(np.abs(a - b) ** 2) * dV(c))) <= 1e-6
+    assert abs(Ea - Eb) <= 1e-7 * abs(Eb)
 
 
 def test_plane_passes_chosen_only_where_they_apply():
