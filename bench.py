@@ -73,9 +73,11 @@ def parse_args():
     ap.add_argument("--quick", action="store_true", help="headline and e2e only")
     ap.add_argument("--only", choices=["batch", "serve", "accuracy", "rot2d", "small2d"],
                     default=None, help="run one auxiliary leg alone and print its JSON")
-    ap.add_argument("--profile", choices=["fp32", "fp64", "fp32_3d", "fp64_3d"], default=None,
+    ap.add_argument("--profile", choices=["fp32", "fp64", "fp32_3d", "fp64_3d", "batch"],
+                    default=None,
                     help="profiling case for ncu: --warmup + --steps time steps of one form "
-                         "(3D: the headline workload; 2D: the rotating case), no timing output")
+                         "(3D: the headline workload; 2D: the rotating case; batch: segments "
+                         "of 100 steps of the 96-solve sweep), no timing output")
     return ap.parse_args()
 
 
@@ -724,6 +726,26 @@ def measured_peak():
 def profile_case(args):
     """Small deterministic run for ncu captures (the timed legs' kernels)."""
     import gpue_b200 as G
+    if args.profile == "batch":
+        # the 96-solve sweep as one batch: one persistent launch per 100-step
+        # segment (checks every 100 steps), default plans
+        cs = batch_cases()
+        ss = [G.Solver(G.make_params(2, c["n"], BATCH["box"], wy=c["wy"], g=c["g"],
+                                     gdt=BATCH["gdt"], precision=G.PREC_FP32)) for c in cs]
+        try:
+            for s, c in zip(ss, cs):
+                s.set_wfc(gauss_start(2, c["n"], BATCH["box"], c["seed"]))
+            with G.Batch(ss) as b:
+                kw = dict(energy_every=BATCH["every"], threshold=BATCH["thr"],
+                          threshold_abs=True)
+                _, st0 = b.evolve(0, 100 * args.warmup + 1, **kw)
+                _, st1 = b.evolve(0, 100 * args.steps, **kw)
+        finally:
+            for s in ss:
+                s.close()
+        print(json.dumps({"profile": "batch", "warmup_launches": st0["kernel_launches"],
+                          "launches": st1["kernel_launches"], "device_ms": st1["device_ms"]}))
+        return
     if args.profile.endswith("_3d"):
         # the headline workload with fixed launch shapes for the z pass (and
         # the x/y line passes of the FP64 form), so a capture does not depend

@@ -410,7 +410,50 @@ gpue_status plan_zpass(gpue_ctx* c, int prec) {
     return GPUE_OK;
 }
 
+gpue_status plan_xy(gpue_ctx* c, int prec) {
+    XYCfg& xc = c->xy[prec];
+    xc.k = nullptr;
+    const char* env = std::getenv("GPUE_XY");
+    if (env && env[0] == '0') return GPUE_OK;
+    if (c->dim != 3 || c->ax[0].n != c->ax[1].n || c->ax[0].n > 256) return GPUE_OK;
+    const XYKernel* k = find_xy_kernel(kprec(prec), c->ax[0].n);
+    EncodeTiled enc = encode_tiled();
+    if (!k || !enc) return GPUE_OK;
+    int max_smem = 0;
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+    if (k->smem > max_smem) return GPUE_OK;
+    int per_sm = 1 << 30;
+    for (const void* fn : {k->fwd, k->inv}) {
+        CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, k->smem));
+        int n = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, k->threads, k->smem));
+        per_sm = std::min(per_sm, n);
+    }
+    if (per_sm < 1) return GPUE_OK;
+    const int n = c->ax[0].n;
+    const cuuint64_t dims[3] = {(cuuint64_t)n, (cuuint64_t)n, (cuuint64_t)c->ax[2].n};
+    const cuuint64_t strides[2] = {(cuuint64_t)n * 8, (cuuint64_t)n * n * 8};
+    const cuuint32_t boxx[3] = {(cuuint32_t)n, 16, 1}, boxy[3] = {16, (cuuint32_t)n, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    for (int w = 0; w < 2; ++w)
+        if (enc(w ? &xc.tmy : &xc.tmx, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, state_of(c, prec),
+                dims, strides, w ? boxy : boxx, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return GPUE_OK;
+    if (!xc.counters) {
+        xc.counter_bytes = 8 + (size_t)c->ax[2].n * sizeof(int);
+        CK(cudaMalloc(&xc.counters, xc.counter_bytes));
+    }
+    const long tiles = 2L * (n / 16) * c->ax[2].n;
+    xc.blocks = (int)std::min<long>((long)per_sm * c->sms, tiles);
+    xc.k = k;
+    return GPUE_OK;
+}
+
 bool plane_ok(const gpue_ctx* c, int prec) {
+    if (c->xy[prec].k && !c->ext)
+        return !(c->p.corotating && (axis_gauge_active(c, 0) || axis_gauge_active(c, 1)));
     if (!c->plane[prec].k || c->ext) return false;
     return !(c->p.corotating && (axis_gauge_active(c, 0) || axis_gauge_active(c, 1)));
 }
@@ -420,7 +463,8 @@ gpue_status make_pass_args(gpue_ctx* c, int prec, const LPass& lp, int gstate, P
     const int ax_i = plane ? 0 : lp.axis;  // the plane passes transform x (and y = x)
     const LaunchCfg& lc = c->lc[prec][ax_i];
     if (plane) {
-        if (!c->plane[prec].k) return fail(c, GPUE_ERR_STATE, "plane passes not planned");
+        if (!c->plane[prec].k && !c->xy[prec].k)
+        return fail(c, GPUE_ERR_STATE, "plane passes not planned");
     } else {
         if (!lc.k) return fail(c, GPUE_ERR_STATE, "axis %d not planned", lp.axis);
         if (lp.red != RED_NONE && lc.ntiles > c->partials_cap - kAuxPartials &&
@@ -499,6 +543,23 @@ gpue_status launch_pass(gpue_ctx* c, int prec, const LPass& lp, int gstate, bool
     gpue_status st = make_pass_args(c, prec, lp, gstate, a);
     if (st) return st;
     a.active = nullptr;  // a single solve always runs
+    if (lp.axis >= kPlaneFwd && c->xy[prec].k) {
+        const XYCfg& xc = c->xy[prec];
+        CK(cudaMemsetAsync(xc.counters, 0, xc.counter_bytes, c->stream));
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(xc.blocks);
+        cfg.blockDim = dim3(xc.k->threads);
+        cfg.dynamicSmemBytes = xc.k->smem;
+        cfg.stream = c->stream;
+        XYCounters kc;
+        kc.ticket = static_cast<unsigned long long*>(xc.counters);
+        kc.done_x = reinterpret_cast<int*>(static_cast<char*>(xc.counters) + 8);
+        void* args[] = {const_cast<CUtensorMap*>(&xc.tmx), const_cast<CUtensorMap*>(&xc.tmy),
+                        &a, &kc};
+        CK(cudaLaunchKernelExC(&cfg, lp.axis == kPlaneFwd ? xc.k->fwd : xc.k->inv, args));
+        c->launches++;
+        return GPUE_OK;
+    }
     if (lp.axis >= kPlaneFwd) {
         const PlaneCfg& pc = c->plane[prec];
         cudaLaunchConfig_t cfg = {};
@@ -1214,6 +1275,7 @@ gpue_status gpue_ctx_create(const gpue_params* p, gpue_ctx** out) {
     }
     st = plan_plane(c, c->prec);
     if (!st) st = plan_zpass(c, c->prec);
+    if (!st) st = plan_xy(c, c->prec);
     if (st) return st;
     const char* tune = std::getenv("GPUE_AUTOTUNE");
     if (tune && tune[0] == '1') {
@@ -1233,6 +1295,8 @@ gpue_status gpue_ctx_destroy(gpue_ctx* c) {
         if (t.buf) cudaFree(t.buf);
     cudaFree(c->psi);
     if (c->psi64) cudaFree(c->psi64);
+    for (auto& x : c->xy)
+        if (x.counters) cudaFree(x.counters);
     if (c->vtab) cudaFree(c->vtab);
     for (auto t : c->atab)
         if (t) cudaFree(t);

@@ -69,6 +69,17 @@ struct PlaneCfg {
 // LPass::axis values of the two plane passes
 enum { kPlaneFwd = 3, kPlaneInv = 4 };
 
+// The cluster-free XY pass of a 3D context (xystream.cuh): the kernel pair,
+// the x-tile and y-tile tensor maps of the resident field and the counters
+// each launch clears first
+struct XYCfg {
+    const XYKernel* k = nullptr;
+    CUtensorMap tmx, tmy;
+    int blocks = 0;
+    void* counters = nullptr;  // ticket (8 bytes) + one int per z-plane
+    size_t counter_bytes = 0;
+};
+
 // The TMA z pass of a 3D context (zpass.cuh): the kernel and the tensor map
 // of the context's resident field
 struct ZCfg {
@@ -116,6 +127,7 @@ struct gpue_ctx {
     gpue_eng::LaunchCfg lc[2][3];       // [precision][axis]
     gpue_eng::PlaneCfg plane[2];        // [precision]: XY-plane passes, if any
     gpue_eng::ZCfg zpass[2];            // [precision]: the TMA z pass, if any
+    gpue_eng::XYCfg xy[2];              // [precision]: the cluster-free XY pass, if any
     bool have_wfc = false;
     bool pending_scale = false;  // scal[kScale] must multiply psi
     std::map<gpue_eng::GraphKey, gpue_eng::Segment> graphs;
@@ -230,6 +242,10 @@ gpue_status plan_plane(gpue_ctx* c, int prec);
 // Plans the TMA z pass of precision prec when the context qualifies (3D, nx a
 // multiple of 16, nz <= 256 with a compiled kernel).
 gpue_status plan_zpass(gpue_ctx* c, int prec);
+// Plans the cluster-free XY pass (3D, nx = ny <= 256 with a compiled kernel);
+// when planned it runs the plane passes of the step instead of the cluster
+// kernels.
+gpue_status plan_xy(gpue_ctx* c, int prec);
 // The plane passes can run this context's steps now (no table or expression
 // fields, no in-plane gauge).
 bool plane_ok(const gpue_ctx* c, int prec);

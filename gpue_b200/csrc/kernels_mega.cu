@@ -94,7 +94,9 @@ __global__ void __launch_bounds__(kMegaThreads, 2) k_batch_mega(const MegaArgs m
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            __threadfence();  // this item's writes (and a finished reduction) first
+            // all threads' writes of this item (ordered by the barrier) and a
+            // finished reduction, before its count
+            __threadfence();
             atomicAdd(m.done + pi, 1);
         }
     }

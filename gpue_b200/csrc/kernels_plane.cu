@@ -3,6 +3,7 @@
 // default radix plan.
 #include "registry.h"
 #include "plane.cuh"
+#include "xystream.cuh"
 #include "zpass.cuh"
 
 namespace gpue {
@@ -36,6 +37,28 @@ static const ZPassKernel kZPassF32[] = {
     GPUE_ZPASS(float, 192, 4, 12, 0, 16),
     GPUE_ZPASS(float, 256, 16, 0, 0, 16),
 };
+
+#define GPUE_XY(T, N, RA, RB, RC, P)                                                        \
+    XYKernel{N, RA, RB, RC, P, XYShape<T, N, RA, RB, P, RC>::THREADS,                        \
+             (int)XYShape<T, N, RA, RB, P, RC>::SMEM,                                        \
+             (const void*)&k_xy<T, N, RA, RB, P, RC, false>,                                 \
+             (const void*)&k_xy<T, N, RA, RB, P, RC, true>}
+
+static const XYKernel kXYF32[] = {
+    GPUE_XY(float, 64, 4, 4, 0, 16),
+    GPUE_XY(float, 96, 4, 6, 0, 8),
+    GPUE_XY(float, 128, 4, 8, 0, 16),
+    GPUE_XY(float, 160, 4, 10, 0, 8),
+    GPUE_XY(float, 192, 4, 12, 0, 16),
+    GPUE_XY(float, 256, 16, 0, 0, 16),
+};
+
+const XYKernel* find_xy_kernel(int prec, int n) {
+    if (prec != PREC_F32) return nullptr;
+    for (const XYKernel& k : kXYF32)
+        if (k.n == n) return &k;
+    return nullptr;
+}
 
 const ZPassKernel* find_zpass_kernel(int prec, int n) {
     if (prec != PREC_F32) return nullptr;

@@ -112,6 +112,12 @@ struct PassArgs {
     int* err;                // plane passes: set non-zero when a bounded wait gave up
 };
 
+// Work counters of the cluster-free XY pass (xystream.cuh).
+struct XYCounters {
+    unsigned long long* ticket;  // zero before the launch
+    int* done_x;                 // [nz] finished x-tiles per plane, zero before the launch
+};
+
 // ------------------------------------------------------- FP64 reductions --
 
 __device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {

@@ -50,6 +50,18 @@ struct ZPassKernel {
 };
 const ZPassKernel* find_zpass_kernel(int prec, int n);
 
+// The cluster-free XY pass pair (xystream.cuh) for 3D fields with nx = ny = n:
+// kernels taking (x-tile tensor map, y-tile tensor map, PassArgs, counters).
+struct XYKernel {
+    int n;
+    int ra, rb, rc, p;
+    int threads;
+    int smem;
+    const void* fwd;
+    const void* inv;
+};
+const XYKernel* find_xy_kernel(int prec, int n);
+
 // The persistent multi-size batched kernel (kernels_mega.cu): the tile body
 // ("kind") of a line length and axis, -1 when the length is not covered;
 // threads per line of a kind; the line stride of its plan; the kernel.

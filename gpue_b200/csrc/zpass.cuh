@@ -34,7 +34,8 @@ struct ZShape {
     static constexpr size_t XCH = (size_t)CX * LSZ * sizeof(cx<T>);
     static constexpr size_t TWB = (size_t)N * 16;
     static constexpr size_t DB = (size_t)N * sizeof(float2);
-    static constexpr size_t SMEM = 2 * TILE + XCH + TWB + DB + 16;
+    // + the two mbarriers, + 128 bytes to align the base for the TMA tiles
+    static constexpr size_t SMEM = 2 * TILE + XCH + TWB + DB + 16 + 128;
     static_assert(std::is_same<T, float>::value, "complex64 z pass");
     static_assert(N <= 256, "a TMA box dimension holds at most 256 elements");
     static_assert(TILE % 128 == 0 && XCH % 16 == 0, "aligned regions");
@@ -51,12 +52,15 @@ __global__ void __launch_bounds__(ZShape<T, N, RA, RB, P, RC>::THREADS, 2)
     using L = typename Z::L;
     constexpr int E = Z::E;
     constexpr int CX = Z::CX;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    cx<T>* land = reinterpret_cast<cx<T>*>(smem_raw);  // [2][N][CX]
-    cx<T>* xch = reinterpret_cast<cx<T>*>(smem_raw + 2 * Z::TILE);
-    float4* tws = reinterpret_cast<float4*>(smem_raw + 2 * Z::TILE + Z::XCH);
-    float2* dz_s = reinterpret_cast<float2*>(smem_raw + 2 * Z::TILE + Z::XCH + Z::TWB);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * Z::TILE + Z::XCH + Z::TWB + Z::DB);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    // TMA tile destinations are 128-byte aligned: align the base here (the
+    // dynamic region follows any static shared variables)
+    unsigned char* smem = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
+    cx<T>* land = reinterpret_cast<cx<T>*>(smem);  // [2][N][CX]
+    cx<T>* xch = reinterpret_cast<cx<T>*>(smem + 2 * Z::TILE);
+    float4* tws = reinterpret_cast<float4*>(smem + 2 * Z::TILE + Z::XCH);
+    float2* dz_s = reinterpret_cast<float2*>(smem + 2 * Z::TILE + Z::XCH + Z::TWB);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * Z::TILE + Z::XCH + Z::TWB + Z::DB);
 
     const int tid = threadIdx.x;
     L::build_stage_table(tws, reinterpret_cast<const float4*>(a.tw), tid, Z::THREADS);
