@@ -361,6 +361,15 @@ using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, 
                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
+// Allocates (once) and clears the work counters of a tile-stream pass.
+gpue_status alloc_counters(gpue_ctx* c, TSCounters& t) {
+    if (t.mem) return GPUE_OK;
+    t.bytes = 16 + (size_t)c->ax[2].n * sizeof(int);
+    CK(cudaMalloc(&t.mem, t.bytes));
+    CK(cudaMemsetAsync(t.mem, 0, t.bytes, c->stream));
+    return GPUE_OK;
+}
+
 EncodeTiled encode_tiled() {
     static EncodeTiled fn = [] {
         void* p = nullptr;
@@ -393,7 +402,8 @@ gpue_status plan_zpass(gpue_ctx* c, int prec) {
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k->fn, k->threads, k->smem));
     if (per_sm < 1) return GPUE_OK;
     // the field as nx x ny x nz elements of 8 bytes (one complex64 each); a
-    // box is 16 x-columns of one y-row over all planes
+    // box is 16 x-columns of one y-row over all planes, landed with the
+    // 128-byte swizzle (its rows are 16 x 8 = 128 bytes)
     const cuuint64_t dims[3] = {(cuuint64_t)c->ax[0].n, (cuuint64_t)c->ax[1].n,
                                 (cuuint64_t)c->ax[2].n};
     const cuuint64_t strides[2] = {(cuuint64_t)c->ax[0].n * 8,
@@ -401,9 +411,11 @@ gpue_status plan_zpass(gpue_ctx* c, int prec) {
     const cuuint32_t box[3] = {16, 1, (cuuint32_t)c->ax[2].n};
     const cuuint32_t estr[3] = {1, 1, 1};
     if (enc(&zc.tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, state_of(c, prec), dims, strides, box,
-            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
             CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return GPUE_OK;
+    gpue_status st = alloc_counters(c, zc.ctr);
+    if (st) return st;
     const long tiles = (long)(c->ax[0].n / 16) * c->ax[1].n;
     zc.blocks = (int)std::min<long>((long)per_sm * c->sms, tiles);
     zc.k = k;
@@ -433,18 +445,20 @@ gpue_status plan_xy(gpue_ctx* c, int prec) {
     const int n = c->ax[0].n;
     const cuuint64_t dims[3] = {(cuuint64_t)n, (cuuint64_t)n, (cuuint64_t)c->ax[2].n};
     const cuuint64_t strides[2] = {(cuuint64_t)n * 8, (cuuint64_t)n * n * 8};
+    // x-tiles: 16 whole rows, as they lie; y-tiles: 16 x-columns over all
+    // y, landed with the 128-byte swizzle (rows of 16 x 8 = 128 bytes)
     const cuuint32_t boxx[3] = {(cuuint32_t)n, 16, 1}, boxy[3] = {16, (cuuint32_t)n, 1};
     const cuuint32_t estr[3] = {1, 1, 1};
     for (int w = 0; w < 2; ++w)
         if (enc(w ? &xc.tmy : &xc.tmx, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, state_of(c, prec),
                 dims, strides, w ? boxy : boxx, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                w ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                CU_TENSOR_MAP_L2_PROMOTION_NONE,
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             return GPUE_OK;
-    if (!xc.counters) {
-        xc.counter_bytes = 8 + (size_t)c->ax[2].n * sizeof(int);
-        CK(cudaMalloc(&xc.counters, xc.counter_bytes));
-    }
+    gpue_status st = alloc_counters(c, xc.ctr);
+    if (st) return st;
+    if (const char* lag = std::getenv("GPUE_XY_LAG")) xc.ctr.lag = std::max(1, std::atoi(lag));
     const long tiles = 2L * (n / 16) * c->ax[2].n;
     xc.blocks = (int)std::min<long>((long)per_sm * c->sms, tiles);
     xc.k = k;
@@ -545,15 +559,17 @@ gpue_status launch_pass(gpue_ctx* c, int prec, const LPass& lp, int gstate, bool
     a.active = nullptr;  // a single solve always runs
     if (lp.axis >= kPlaneFwd && c->xy[prec].k) {
         const XYCfg& xc = c->xy[prec];
-        CK(cudaMemsetAsync(xc.counters, 0, xc.counter_bytes, c->stream));
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(xc.blocks);
         cfg.blockDim = dim3(xc.k->threads);
         cfg.dynamicSmemBytes = xc.k->smem;
         cfg.stream = c->stream;
-        XYCounters kc;
-        kc.ticket = static_cast<unsigned long long*>(xc.counters);
-        kc.done_x = reinterpret_cast<int*>(static_cast<char*>(xc.counters) + 8);
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = pdl ? 1 : 0;
+        XYCounters kc = xc.ctr.dev();
         void* args[] = {const_cast<CUtensorMap*>(&xc.tmx), const_cast<CUtensorMap*>(&xc.tmy),
                         &a, &kc};
         CK(cudaLaunchKernelExC(&cfg, lp.axis == kPlaneFwd ? xc.k->fwd : xc.k->inv, args));
@@ -594,7 +610,9 @@ gpue_status launch_pass(gpue_ctx* c, int prec, const LPass& lp, int gstate, bool
         at[0].val.programmaticStreamSerializationAllowed = 1;
         cfg.attrs = at;
         cfg.numAttrs = pdl ? 1 : 0;
-        void* args[] = {const_cast<CUtensorMap*>(&zc.tm), &a};
+        XYCounters kc = zc.ctr.dev();
+        void* args[] = {const_cast<CUtensorMap*>(&zc.tm), const_cast<CUtensorMap*>(&zc.tm), &a,
+                        &kc};
         CK(cudaLaunchKernelExC(&cfg, zc.k->fn, args));
         c->launches++;
         return GPUE_OK;
@@ -1296,7 +1314,9 @@ gpue_status gpue_ctx_destroy(gpue_ctx* c) {
     cudaFree(c->psi);
     if (c->psi64) cudaFree(c->psi64);
     for (auto& x : c->xy)
-        if (x.counters) cudaFree(x.counters);
+        if (x.ctr.mem) cudaFree(x.ctr.mem);
+    for (auto& z : c->zpass)
+        if (z.ctr.mem) cudaFree(z.ctr.mem);
     if (c->vtab) cudaFree(c->vtab);
     for (auto t : c->atab)
         if (t) cudaFree(t);

@@ -69,23 +69,39 @@ struct PlaneCfg {
 // LPass::axis values of the two plane passes
 enum { kPlaneFwd = 3, kPlaneInv = 4 };
 
-// The cluster-free XY pass of a 3D context (xystream.cuh): the kernel pair,
-// the x-tile and y-tile tensor maps of the resident field and the counters
-// each launch clears first
+// Work counters of a tile-stream pass (tstream.cuh): ticket (8 bytes),
+// finish count (4 bytes, padded to 8), one int per z-plane; cleared once at
+// allocation, then by each launch's last CTA
+struct TSCounters {
+    void* mem = nullptr;
+    size_t bytes = 0;
+    int lag = 64;  // XY pass: planes between a plane's x-tiles and its y-tiles
+    XYCounters dev() const {
+        XYCounters k;
+        k.lag = lag;
+        k.ticket = static_cast<unsigned long long*>(mem);
+        k.finish = reinterpret_cast<unsigned*>(static_cast<char*>(mem) + 8);
+        k.done_x = reinterpret_cast<int*>(static_cast<char*>(mem) + 16);
+        return k;
+    }
+};
+
+// The XY pass of a 3D context (tstream.cuh): the kernel pair, the x-tile and
+// y-tile tensor maps of the resident field and the work counters
 struct XYCfg {
     const XYKernel* k = nullptr;
     CUtensorMap tmx, tmy;
     int blocks = 0;
-    void* counters = nullptr;  // ticket (8 bytes) + one int per z-plane
-    size_t counter_bytes = 0;
+    TSCounters ctr;
 };
 
-// The TMA z pass of a 3D context (zpass.cuh): the kernel and the tensor map
-// of the context's resident field
+// The TMA z pass of a 3D context (tstream.cuh): the kernel, the z-tile tensor
+// map of the context's resident field and the work counters
 struct ZCfg {
     const ZPassKernel* k = nullptr;
     CUtensorMap tm;
     int blocks = 0;
+    TSCounters ctr;
 };
 
 struct GraphKey {

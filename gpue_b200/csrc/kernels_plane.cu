@@ -1,10 +1,10 @@
-// kernels_plane.cu -- the complex64 XY-plane pass kernels (plane.cuh) and the
-// TMA z pass (zpass.cuh) for the 3D step, per length with the line length's
-// default radix plan.
+// kernels_plane.cu -- the complex64 pass kernels of the 3D step beyond the
+// line passes: the cluster XY-plane passes (plane.cuh) and the TMA tile-stream
+// XY and z passes (tstream.cuh), per length with the line length's default
+// radix plan.
 #include "registry.h"
 #include "plane.cuh"
-#include "xystream.cuh"
-#include "zpass.cuh"
+#include "tstream.cuh"
 
 namespace gpue {
 
@@ -25,9 +25,9 @@ static const PlaneKernel kPlanesF32[] = {
 };
 
 #define GPUE_ZPASS(T, N, RA, RB, RC, P)                                                     \
-    ZPassKernel{N, RA, RB, RC, P, ZShape<T, N, RA, RB, P, RC>::THREADS,                      \
-                (int)ZShape<T, N, RA, RB, P, RC>::SMEM,                                      \
-                (const void*)&k_zpass<T, N, RA, RB, P, RC>}
+    ZPassKernel{N, RA, RB, RC, P, TSShape<T, N, RA, RB, P, RC>::THREADS,                     \
+                (int)TSShape<T, N, RA, RB, P, RC>::SMEM,                                     \
+                (const void*)&k_tstream<T, N, RA, RB, P, RC, TS_Z>}
 
 static const ZPassKernel kZPassF32[] = {
     GPUE_ZPASS(float, 64, 4, 4, 0, 16),
@@ -39,10 +39,10 @@ static const ZPassKernel kZPassF32[] = {
 };
 
 #define GPUE_XY(T, N, RA, RB, RC, P)                                                        \
-    XYKernel{N, RA, RB, RC, P, XYShape<T, N, RA, RB, P, RC>::THREADS,                        \
-             (int)XYShape<T, N, RA, RB, P, RC>::SMEM,                                        \
-             (const void*)&k_xy<T, N, RA, RB, P, RC, false>,                                 \
-             (const void*)&k_xy<T, N, RA, RB, P, RC, true>}
+    XYKernel{N, RA, RB, RC, P, TSShape<T, N, RA, RB, P, RC>::THREADS,                        \
+             (int)TSShape<T, N, RA, RB, P, RC>::SMEM,                                        \
+             (const void*)&k_tstream<T, N, RA, RB, P, RC, TS_XY_FWD>,                        \
+             (const void*)&k_tstream<T, N, RA, RB, P, RC, TS_XY_INV>}
 
 static const XYKernel kXYF32[] = {
     GPUE_XY(float, 64, 4, 4, 0, 16),

@@ -112,10 +112,13 @@ struct PassArgs {
     int* err;                // plane passes: set non-zero when a bounded wait gave up
 };
 
-// Work counters of the cluster-free XY pass (xystream.cuh).
+// Work counters of the TMA tile-stream passes (tstream.cuh); zero between
+// launches (the last CTA of each launch clears them).
 struct XYCounters {
-    unsigned long long* ticket;  // zero before the launch
-    int* done_x;                 // [nz] finished x-tiles per plane, zero before the launch
+    unsigned long long* ticket;  // next ticket
+    unsigned* finish;            // CTAs finished
+    int* done_x;                 // [nz] x-tiles stored per plane (XY pass)
+    int lag;                     // XY pass: planes between a plane's x-tiles and y-tiles
 };
 
 // ------------------------------------------------------- FP64 reductions --

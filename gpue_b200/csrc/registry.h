@@ -38,9 +38,10 @@ struct PlaneKernel {
 // nullptr when no plane pass is compiled for (precision, n)
 const PlaneKernel* find_plane_kernel(int prec, int n);
 
-// The TMA z pass (zpass.cuh) for 3D fields with nz = n: tiles of 16 x-columns,
-// `threads` threads and `smem` bytes per CTA; its first parameter is the
-// CUtensorMap of the field (passed as void* here to keep cuda.h out).
+// The TMA z pass (tstream.cuh) for 3D fields with nz = n: tiles of 16
+// x-columns, `threads` threads and `smem` bytes per CTA; a kernel taking
+// (z-tile tensor map, unused tensor map, PassArgs, counters) (passed as void*
+// here to keep cuda.h out).
 struct ZPassKernel {
     int n;
     int ra, rb, rc, p;
@@ -50,8 +51,8 @@ struct ZPassKernel {
 };
 const ZPassKernel* find_zpass_kernel(int prec, int n);
 
-// The cluster-free XY pass pair (xystream.cuh) for 3D fields with nx = ny = n:
-// kernels taking (x-tile tensor map, y-tile tensor map, PassArgs, counters).
+// The XY pass pair (tstream.cuh) for 3D fields with nx = ny = n: kernels
+// taking (x-tile tensor map, y-tile tensor map, PassArgs, counters).
 struct XYKernel {
     int n;
     int ra, rb, rc, p;

@@ -3,9 +3,9 @@ five-pass line schedule.
 
 A 3D FP32 context with nx = ny of a length that has an XY kernel runs its
 steps as XY[scale V/2 Fx Fy] Z[Fz K Iz] XY[Ix Iy V/2 norm], by the
-cluster-free XY stream kernel (xystream.cuh; GPUE_XY=0 turns it off) or the
+TMA tile-stream XY kernel (tstream.cuh; GPUE_XY=0 turns it off) or the
 cluster plane kernel (plane.cuh; GPUE_PLANE=0 turns it off), with the TMA z
-pass (zpass.cuh; GPUE_ZTMA=0 turns it off).  Both schedules are the same
+pass (tstream.cuh; GPUE_ZTMA=0 turns it off).  Both schedules are the same
 arithmetic in another order, so they agree to complex64 round-off; both are
 checked against the FP64 oracle with the FP32 tolerances of the other parity
 tests (wavefunction L2 <= 1e-5, relative energy <= 1e-5).
