@@ -59,6 +59,19 @@ __device__ __forceinline__ cx<T> cconj(cx<T> a) { return {a.x, -a.y}; }
 template <typename T>
 __device__ __forceinline__ cx<T> mul_mi(cx<T> a) { return {a.y, -a.x}; }
 
+// Complex64 sums and differences as packed FP32x2 operations (sm_100: one
+// instruction for both components).  Each component is rounded exactly as
+// the scalar operation rounds it (a - b is formed as b * -1 + a, whose
+// product is exact), so results do not change, only the instruction count.
+__device__ __forceinline__ float2 f2(cx<float> a) { return make_float2(a.x, a.y); }
+__device__ __forceinline__ cx<float> c2(float2 a) { return {a.x, a.y}; }
+__device__ __forceinline__ cx<float> operator+(cx<float> a, cx<float> b) {
+    return c2(__fadd2_rn(f2(a), f2(b)));
+}
+__device__ __forceinline__ cx<float> operator-(cx<float> a, cx<float> b) {
+    return c2(__ffma2_rn(f2(b), make_float2(-1.f, -1.f), f2(a)));
+}
+
 // Complex64 twiddles are carried as a pair of floats, hi + lo, equal to the
 // FP64 twiddle to about 2^-48.  A single rounded float has |W|^2 = 1 - O(1e-8)
 // on average (the rounding of cos and sin is not magnitude-neutral), which
@@ -73,6 +86,17 @@ __device__ __forceinline__ cx<float> cmul_split(cx<float> a, cx<float> hi, cx<fl
     const float tx = fmaf(a.x, lo.x, -a.y * lo.y);
     const float ty = fmaf(a.x, lo.y, a.y * lo.x);
     return {fmaf(a.x, hi.x, fmaf(-a.y, hi.y, tx)), fmaf(a.x, hi.y, fmaf(a.y, hi.x, ty))};
+}
+// The same product for a constant twiddle, as four packed FP32x2 operations
+// in the same order (bit-identical to cmul_split): the constant pairs
+// (lo.x, lo.y), (-lo.y, lo.x), (-hi.y, hi.x), (hi.x, hi.y) need no shuffling
+__device__ __forceinline__ cx<float> cmul_split_const(cx<float> a, float hx, float hy, float lx,
+                                                      float ly) {
+    const float2 ax = make_float2(a.x, a.x), ay = make_float2(a.y, a.y);
+    float2 t = __fmul2_rn(ay, make_float2(-ly, lx));
+    t = __ffma2_rn(ax, make_float2(lx, ly), t);
+    t = __ffma2_rn(ay, make_float2(-hy, hx), t);
+    return c2(__ffma2_rn(ax, make_float2(hx, hy), t));
 }
 
 // a * W_R^m, W_R = exp(-2 pi i / R), with exact shortcuts at multiples of pi/2
@@ -91,7 +115,7 @@ __device__ __forceinline__ cx<T> tw_const(cx<T> a) {
         constexpr double c = tw_cos(R, m), s = -tw_sin(R, m);
         constexpr float ch = (float)c, sh = (float)s;
         constexpr float cl = (float)(c - (double)ch), sl = (float)(s - (double)sh);
-        return cmul_split(a, cx<float>{ch, sh}, cx<float>{cl, sl});
+        return cmul_split_const(a, ch, sh, cl, sl);
     } else if constexpr (8 * m == R || 8 * m == 3 * R || 8 * m == 5 * R || 8 * m == 7 * R) {
         constexpr T h = (T)0.70710678118654752440;
         constexpr double c = tw_cos(R, m);
@@ -145,6 +169,20 @@ struct SmallDFT<4, T> {
         v[1] = d02 + d13;
         v[2] = s02 - s13;
         v[3] = d02 - d13;
+    }
+};
+
+// Complex64: the four sums and differences packed, the -i products as scalar
+// component sums (the same values as the generic form)
+template <>
+struct SmallDFT<4, float> {
+    static __device__ __forceinline__ void run(cx<float>* v) {
+        const cx<float> s02 = v[0] + v[2], d02 = v[0] - v[2];
+        const cx<float> s13 = v[1] + v[3], d13 = v[1] - v[3];
+        v[0] = s02 + s13;
+        v[2] = s02 - s13;
+        v[1] = {d02.x + d13.y, d02.y - d13.x};
+        v[3] = {d02.x - d13.y, d02.y + d13.x};
     }
 };
 

@@ -23,8 +23,9 @@
 //
 // XY ordering.  Tickets follow: the x-tiles of plane g, then the y-tiles of
 // plane g - LAG, for g = 0, 1, ...  A y-tile of plane z may load only after
-// all x-tiles of plane z are stored (a per-plane count, raised by each
-// x-tile's producer once its store is complete); by then the plane is
+// all x-tiles of plane z are stored (a per-plane count, raised with release
+// semantics by each x-tile's producer once its store is complete, and read
+// with acquire semantics); by then the plane is
 // normally still in L2, so the field crosses HBM once in and once out.  The
 // count of an x-tile is raised one store later (when the next store is
 // issued, the previous one is complete or nearly so), so the producer rarely
@@ -95,19 +96,20 @@ __device__ __forceinline__ int sw128(int r, int c) {
     return r * 16 + ((((c >> 1) ^ (r & 7)) << 1) | (c & 1));
 }
 
-// XY ticket t -> (kind, plane, tile): xi x-tiles and yi y-tiles per plane.
-__device__ __forceinline__ int xy_ticket(long t, int xi, int yi, int nz, int lag, int& z,
-                                         int& tile) {
-    const long t1 = (long)lag * xi, t2 = t1 + (long)(nz - lag) * (xi + yi);
+// XY ticket t -> (kind, plane, tile): xi x-tiles and yi y-tiles per plane
+// (32-bit arithmetic: a launch has nz * (xi + yi) < 2^31 tiles).
+__device__ __forceinline__ int xy_ticket(unsigned t, unsigned xi, unsigned yi, unsigned nz,
+                                         unsigned lag, int& z, int& tile) {
+    const unsigned t1 = lag * xi, t2 = t1 + (nz - lag) * (xi + yi);
     if (t < t1) {
         z = (int)(t / xi);
         tile = (int)(t % xi);
         return TILE_X;
     }
     if (t < t2) {
-        const long u = t - t1;
+        const unsigned u = t - t1;
         const int w = (int)(u % (xi + yi));
-        const int g = lag + (int)(u / (xi + yi));
+        const int g = (int)(lag + u / (xi + yi));
         if (w < xi) {
             z = g;
             tile = w;
@@ -117,10 +119,21 @@ __device__ __forceinline__ int xy_ticket(long t, int xi, int yi, int nz, int lag
         tile = w - xi;
         return TILE_Y;
     }
-    const long u = t - t2;
-    z = nz - lag + (int)(u / yi);
+    const unsigned u = t - t2;
+    z = (int)(nz - lag + u / yi);
     tile = (int)(u % yi);
     return TILE_Y;
+}
+
+// The x-tile count of a plane, read with acquire semantics (the stores it
+// counts happen before what follows), and raised with release semantics.
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void red_release_add(int* p, int v) {
+    asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* b) {
@@ -204,16 +217,15 @@ __global__ void __launch_bounds__(TSShape<T, N, RA, RB, P, RC>::THREADS, 2)
                 return z < 256 && ((s_ready[z >> 5] >> (z & 31)) & 1u);
             };
             auto see_ready = [&](int z) {
-                // the other CTAs' stores of this plane before TMA reads of it
-                __threadfence();
+                // (after an acquire read of the count) the other CTAs' stores
+                // of this plane before TMA reads of it
                 asm volatile("fence.proxy.async.global;" ::: "memory");
                 if (z < 256) s_ready[z >> 5] |= 1u << (z & 31);
             };
             auto count = [&](int z) {
                 // the store is complete: publish it to the y-tiles of plane z
                 asm volatile("fence.proxy.async.global;" ::: "memory");
-                __threadfence();
-                atomicAdd(k.done_x + z, 1);
+                red_release_add(k.done_x + z, 1);
             };
             auto flush = [&] {
                 asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
@@ -257,14 +269,14 @@ __global__ void __launch_bounds__(TSShape<T, N, RA, RB, P, RC>::THREADS, 2)
                 }
                 if constexpr (KIND == TS_Z) {
                     m.kind = TILE_Z;
-                    m.z = (int)(m.tk / yi);
-                    m.tile = (int)(m.tk % yi);
+                    m.z = (int)((unsigned)m.tk / (unsigned)yi);
+                    m.tile = (int)((unsigned)m.tk % (unsigned)yi);
                 } else {
-                    m.kind = xy_ticket(m.tk, xi, yi, nz, lag, m.z, m.tile);
+                    m.kind = xy_ticket((unsigned)m.tk, xi, yi, nz, lag, m.z, m.tile);
                 }
                 slot[b] = make_int4(m.kind, m.z, m.tile, 0);
                 if (m.kind == TILE_Y && !known_ready(m.z)) {
-                    if (*reinterpret_cast<const volatile int*>(k.done_x + m.z) < xi) {
+                    if (ld_acquire(k.done_x + m.z) < xi) {
                         m.pend = true;
                         return;
                     }
@@ -280,9 +292,8 @@ __global__ void __launch_bounds__(TSShape<T, N, RA, RB, P, RC>::THREADS, 2)
                 if (m.pend) {
                     // everything held with a smaller ticket is stored and counted
                     flush();
-                    const volatile int* d = k.done_x + m.z;
                     unsigned polls = 0;
-                    while (*d < xi) {
+                    while (ld_acquire(k.done_x + m.z) < xi) {
                         if (++polls >= kPlaneWaitPolls) {
                             ok = false;
                             break;
@@ -306,17 +317,18 @@ __global__ void __launch_bounds__(TSShape<T, N, RA, RB, P, RC>::THREADS, 2)
                     "r"(c0), "r"(c1), "r"(c2), "r"(smem_addr(land + (size_t)b * N * LT))
                     : "memory");
                 asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-                if (unsig >= 0) {
-                    // the store before this one is complete
-                    asm volatile("cp.async.bulk.wait_group 1;" ::: "memory");
-                    count(unsig);
-                    unsig = -1;
-                }
-                if (m.kind == TILE_X) unsig = m.z;
+                const int stored_x = m.kind == TILE_X ? m.z : -1;
+                // refill the buffer first: the compute warps wait for it
                 asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
                 m.tk = (long)nxt;
                 prepare(bc, m);
                 if (m.tk < total) nxt = atomicAdd(k.ticket, 1ull);
+                if (unsig >= 0) {
+                    // the store before this one is complete
+                    asm volatile("cp.async.bulk.wait_group 1;" ::: "memory");
+                    count(unsig);
+                }
+                unsig = stored_x;
                 return true;
             };
             using I0 = std::integral_constant<int, 0>;
