@@ -209,6 +209,8 @@ def lib():
         L.gpue_get_plan.argtypes = [vp, i32, C.POINTER(PlanInfo)]
         L.gpue_list_plans.argtypes = [i32, i32, C.POINTER(PlanInfo), i32, C.POINTER(i32)]
         L.gpue_set_plan.argtypes = [vp, i32, i32, i32, i32, i32, i32]
+        L.gpue_time_passes.argtypes = [vp, i32, i32, C.POINTER(C.c_float), C.POINTER(i32), i32,
+                                       C.POINTER(i32)]
         L.gpue_server_create.argtypes = [C.POINTER(ServerOpts), C.POINTER(vp)]
         L.gpue_server_destroy.argtypes = [vp]
         L.gpue_server_last_error.argtypes = [vp]
@@ -232,7 +234,7 @@ def lib():
                      "gpue_get_plan", "gpue_set_gauge_tables", "gpue_observables_get",
                      "gpue_find_vortices", "gpue_set_potential_table", "gpue_snapshot_save",
                      "gpue_snapshot_load", "gpue_list_plans", "gpue_set_plan",
-                     "gpue_set_check_observables"):
+                     "gpue_set_check_observables", "gpue_time_passes"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -425,6 +427,17 @@ class Solver:
         """Use one compiled plan on one axis (gpue_set_plan)."""
         self._ck(lib().gpue_set_plan(self._h, axis, ra, rb, rc, threads_per_line,
                                      lines_per_cta))
+
+    def time_passes(self, gstate=0, nsteps=8):
+        """Mean device time (us) of each pass of a time step (gpue_time_passes),
+        as a list of (kind, us): kind 0/1/2 a line pass along x/y/z (2 also the
+        3D complex64 z tile pass), 3/4 the forward/inverse XY pass."""
+        cap = 16
+        us = (C.c_float * cap)()
+        kinds = (C.c_int32 * cap)()
+        n = C.c_int32(0)
+        self._ck(lib().gpue_time_passes(self._h, gstate, nsteps, us, kinds, cap, C.byref(n)))
+        return [(int(kinds[i]), float(us[i])) for i in range(min(n.value, cap))]
 
     def plan(self, axis):
         out = PlanInfo()

@@ -1066,6 +1066,62 @@ struct LoopOut {
 
 // The step loop of evolve() on the state of precision `prec`, absolute steps
 // [off, off + nsteps), energy checks and early stop as GPUE does them.
+// Mean device time of each pass of a step (gpue_time_passes).
+gpue_status time_passes(gpue_ctx* c, int prec, int gstate, int nsteps, std::vector<float>& us,
+                        std::vector<int>& kinds) {
+    gpue_status st = build_tables(c, prec, gstate);
+    if (st) return st;
+    if (!c->have_wfc)  // any finite state times the same; this one is ~1e-2 (FP32)
+        CK(cudaMemsetAsync(state_of(c, prec), 0x3C, c->N * elem_size(prec), c->stream));
+    double saved[kNScal];
+    const size_t bytes = c->N * elem_size(prec);
+    CK(cudaMemcpyAsync(c->scratch, state_of(c, prec), bytes, cudaMemcpyDeviceToDevice,
+                       c->stream));
+    CK(cudaMemcpyAsync(saved, c->scal, sizeof saved, cudaMemcpyDeviceToHost, c->stream));
+    const long launches = c->launches;
+    const bool plane = plane_ok(c, prec);
+    std::vector<std::vector<float>> per;  // [step][pass] ms
+    std::vector<cudaEvent_t> ev;
+    for (int i = 0; i < nsteps && !st; ++i) {
+        std::vector<LPass> v;
+        step_passes(c, i, gstate, i == 0 ? (gstate == 0 && c->pending_scale) : gstate == 0,
+                    1.0, 0, v, plane);
+        fuse(v);
+        if (i == 0) {
+            kinds.clear();
+            for (const LPass& lp : v) kinds.push_back(lp.axis);
+            ev.assign(v.size() + 1, nullptr);
+            for (cudaEvent_t& e : ev)
+                if (cudaEventCreate(&e) != cudaSuccess) st = GPUE_ERR_CUDA;
+            if (st) break;
+        }
+        if (v.size() + 1 != ev.size()) break;  // a step of another shape: stop here
+        std::vector<float> ms(v.size(), 0.f);
+        if (cudaEventRecord(ev[0], c->stream) != cudaSuccess) st = GPUE_ERR_CUDA;
+        for (size_t k = 0; k < v.size() && !st; ++k) {
+            st = launch_pass(c, prec, v[k], gstate, false);
+            if (!st && cudaEventRecord(ev[k + 1], c->stream) != cudaSuccess) st = GPUE_ERR_CUDA;
+        }
+        if (!st && cudaEventSynchronize(ev.back()) != cudaSuccess) st = GPUE_ERR_CUDA;
+        for (size_t k = 0; k < v.size() && !st; ++k)
+            if (cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]) != cudaSuccess) st = GPUE_ERR_CUDA;
+        per.push_back(ms);
+    }
+    for (cudaEvent_t e : ev)
+        if (e) cudaEventDestroy(e);
+    c->launches = launches;
+    // the state and the scalars as they were, whatever happened above
+    CK(cudaMemcpyAsync(state_of(c, prec), c->scratch, bytes, cudaMemcpyDeviceToDevice,
+                       c->stream));
+    CK(cudaMemcpyAsync(c->scal, saved, sizeof saved, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (st) return fail(c, st, "gpue_time_passes: a launch or an event failed");
+    us.assign(kinds.size(), 0.f);
+    for (const auto& ms : per)
+        for (size_t k = 0; k < ms.size() && k < us.size(); ++k) us[k] += ms[k] * 1e3f / per.size();
+    return GPUE_OK;
+}
+
 gpue_status step_loop(gpue_ctx* c, int prec, int off, int nsteps, int gstate,
                       const gpue_evolve_opts& o, int guard, LoopOut& lo) {
     const int last = off + nsteps;
@@ -1700,6 +1756,23 @@ gpue_status gpue_autotune(gpue_ctx* c, int32_t flags) {
     CK(cudaSetDevice(c->device));
     CK(cudaStreamSynchronize(c->stream));
     return autotune_ctx(c, c->prec, (flags & 1) != 0);
+}
+
+gpue_status gpue_time_passes(gpue_ctx* c, int32_t gstate, int32_t nsteps, float* us,
+                             int32_t* kinds, int32_t cap, int32_t* npass) {
+    if (!c || !npass || nsteps < 1 || cap < 0 || (cap > 0 && (!us || !kinds)) ||
+        (gstate != 0 && gstate != 1))
+        return GPUE_ERR_INVALID_ARG;
+    std::vector<float> t;
+    std::vector<int> k;
+    gpue_status st = time_passes(c, c->prec, gstate, nsteps, t, k);
+    if (st) return st;
+    *npass = (int32_t)t.size();
+    for (int i = 0; i < cap && i < (int)t.size(); ++i) {
+        us[i] = t[i];
+        kinds[i] = k[i];
+    }
+    return GPUE_OK;
 }
 
 gpue_status gpue_get_plan(gpue_ctx* c, int32_t axis, gpue_plan_info* out) {

@@ -336,6 +336,19 @@ gpue_status gpue_get_plan(gpue_ctx* ctx, int32_t axis, gpue_plan_info* out);
 gpue_status gpue_list_plans(int32_t precision, int32_t n, gpue_plan_info* out, int32_t cap,
                             int32_t* count);
 
+/* No counterpart in GPUE: the device time of each pass of a time step of the
+ * context's schedule for gstate's time kind.  nsteps steps are run on the
+ * state with a CUDA event pair around every pass launch (on the context's
+ * stream, so no launch overlaps the next), and then undone: the state and the
+ * scalar slots are saved first and put back after.  us[i] receives the mean
+ * duration of pass i of a step, kinds[i] what the pass is: 0, 1, 2 a line
+ * pass along x, y, z (2 also the z tile pass of a 3D complex64 step), 3 and
+ * 4 the forward and inverse XY pass of a 3D complex64 step.  *npass receives
+ * the passes per step; at most cap entries are written.  A measurement aid:
+ * the results of later calls do not change. */
+gpue_status gpue_time_passes(gpue_ctx* ctx, int32_t gstate, int32_t nsteps, float* us,
+                             int32_t* kinds, int32_t cap, int32_t* npass);
+
 /* Use the compiled plan (ra, rb, rc, threads_per_line) on one axis of the
  * context, with lines_per_cta lines per CTA (0: the default count).  Fails
  * with GPUE_ERR_INVALID_ARG when no such plan exists or the launch shape does

@@ -98,3 +98,31 @@ def test_plane_passes_chosen_only_where_they_apply():
     lines, El, rl = run(c, 6, 1, "lines", psi0)
     assert r["kernel_launches"] == rl["kernel_launches"]
     assert np.array_equal(got, lines)
+
+
+@pytest.mark.parametrize("gstate", [0, 1], ids=["imag", "real"])
+def test_time_passes_reports_the_step_and_leaves_the_state(gstate):
+    """gpue_time_passes on a 3D complex64 grid: the three passes of the step
+    (forward XY, z, inverse XY), each with a positive device time, and the
+    state afterwards exactly as before; a later evolve matches one on a
+    context that was never timed (to round-off: the norm's partial sums
+    follow the tile tickets, which change from launch to launch)."""
+    import gpue_b200 as G
+    c = dict(cases.DEFAULTS, dim=3, n=64, box=8.0, wz=2.5, g=200.0, gdt=1e-4, dt=1e-4,
+             seed=77, init="gauss" if gstate == 0 else "phase", energy_every=4)
+    psi0 = cases.initial_psi(c)
+    with G.Solver(product_params(c, G.PREC_FP32)) as s, \
+            G.Solver(product_params(c, G.PREC_FP32)) as u:
+        s.set_wfc(psi0)
+        u.set_wfc(psi0)
+        s.evolve(2, gstate)
+        u.evolve(2, gstate)
+        before = s.get_wfc()
+        t = s.time_passes(gstate, nsteps=4)
+        assert [k for k, _ in t] == [3, 2, 4]
+        assert all(us > 0 for _, us in t)
+        assert np.array_equal(s.get_wfc(), before)
+        s.evolve(4, gstate, step_offset=2)
+        u.evolve(4, gstate, step_offset=2)
+        a, b = s.get_wfc(), u.get_wfc()
+        assert np.max(np.abs(a - b)) <= 1e-6 * np.max(np.abs(b))
