@@ -827,8 +827,11 @@ def main():
             ms, launches, clocks = timed_steps(G, torch, s, args.steps, args.warmup, dev,
                                                barrier, 0, sampler=sampler)
             E = s.energy()
+            # each pass kernel of a step timed alone (event pair per launch on
+            # the library's stream, state restored), after the timed region
+            passes = s.time_passes(0, nsteps=8)
         ms = replicas.max_over_ranks(ms, dist, dev)
-        res[name] = dict(ms=ms, launches=launches, clocks=clocks, E=E)
+        res[name] = dict(ms=ms, launches=launches, clocks=clocks, E=E, passes=passes)
 
     tsteps = args.steps * STEPS_PER_BENCH_STEP
     v32 = world * pts * tsteps / (res["fp32"]["ms"] * 1e-3)
@@ -841,31 +844,41 @@ def main():
             dist.destroy_process_group()
         return
 
-    # roofline of the dominant kernel, the XY-plane pass: one launch reads and
-    # writes the complex64 field once (2 * 8 bytes per point); its duration is
-    # taken as the step time over the 3 pass launches per step
+    # roofline of the dominant kernel: of the step's pass kernels (each reads
+    # and writes the complex64 field once: 2 * 8 bytes per point), the one
+    # with the longest duration, timed alone on the library's stream
     per_time_step_s = res["fp32"]["ms"] * 1e-3 / tsteps
-    pass_s = per_time_step_s / PASSES["fp32"]
-    achieved = 2 * 8 * pts / pass_s / 1e9
+    kind_names = {0: "x line pass", 1: "y line pass", 2: "z tile pass (Fz K Iz)",
+                  3: "forward XY tile pass ([scale] V/2 Fx Fy)",
+                  4: "inverse XY tile pass (Ix Iy V/2 norm)"}
+    passes = res["fp32"]["passes"]
+    dom_kind, dom_us = max(passes, key=lambda kv: kv[1])
+    achieved = 2 * 8 * pts / (dom_us * 1e-6) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get("head_fp32_plane_pass_bytes_per_launch")
+            traffic = json.load(open(tpath)).get("head_fp32_dominant_pass_bytes_per_launch")
         except Exception:
             traffic = None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
+                "kernel": kind_names.get(dom_kind, str(dom_kind)),
+                "kernel_us": dom_us,
+                "passes_us": [[kind_names.get(k, str(k)), us] for k, us in passes],
                 "peak_source": (peak_src + " (MEASURED_PEAKS.json hbm_gbs)")
                 if peak_src == "measured" else "fallback 6.65 TB/s",
+                "step_frac_48B": 48 * pts / per_time_step_s / 1e9 / peak,
                 "alg_frac_80B": 80 * pts / per_time_step_s / 1e9 / peak,
-                "note": "achieved = 256 MiB algorithmic bytes per pass launch (read+write of "
-                        "the complex64 field) / mean pass duration (the bench step time over "
-                        "its 3 x 100 pass launches, CUDA events on the library's stream); "
-                        "alg_frac_80B counts 80 B per point and step (the five-pass line "
-                        "schedule) against the same peak; traffic is dram read+write bytes "
-                        "per launch of the plane pass from an ncu capture "
-                        "(profiles/traffic.json), not measured in this run"}
+                "note": "achieved = 256 MiB algorithmic bytes per launch (one read and one "
+                        "write of the complex64 field) / the dominant pass kernel's mean "
+                        "duration, timed with CUDA events on the library's stream after the "
+                        "timed region (gpue_time_passes: 8 steps, one event pair per launch); "
+                        "step_frac_48B counts the three-pass step's 48 B per point against "
+                        "the bench step time, alg_frac_80B the five-pass line schedule's "
+                        "80 B per point; traffic = dram read+write bytes per launch of that "
+                        "kernel from an ncu capture (profiles/traffic.json), not measured "
+                        "in this run"}
 
     # rank 0 alone; the CPU baseline and the extra legs only at N = 1
     cpu = None

@@ -465,6 +465,26 @@ __device__ __forceinline__ void op_kphase_f32(cx<float> (&v)[L::E], int t, const
     }
 }
 
+// The same, with the k factors as (d.x, d.y, d.y, d.x) and the product of
+// the line and k factors (dmul) and the real scaling as packed FP32x2
+// operations in dmul's order: bit-identical to op_kphase_f32.
+template <class L>
+__device__ __forceinline__ void op_kphase_f32_packed(cx<float> (&v)[L::E], int t,
+                                                     const float4* dk, float2 dl, float s) {
+    const float2 lneg = make_float2(-dl.y, dl.y), lx = make_float2(dl.x, dl.x);
+    const float2 ss = make_float2(s, s);
+#pragma unroll
+    for (int e = 0; e < L::E; ++e) {
+        const float4 q = dk[L::index(t, e)];
+        float2 d = __fadd2_rn(dl, make_float2(q.x, q.y));
+        d = __ffma2_rn(lneg, make_float2(q.z, q.w), d);
+        d = __ffma2_rn(lx, make_float2(q.x, q.y), d);
+        const cx<float> w = dapply(v[e], d);
+        const float2 r = __fmul2_rn(make_float2(w.x, w.y), ss);
+        v[e] = {r.x, r.y};
+    }
+}
+
 // OP_NORM, complex64: the thread's |psi|^2 summed in FP32 (relative error
 // ~E 2^-24 per thread, unbiased), entering the FP64 compensated sum once
 template <int E>

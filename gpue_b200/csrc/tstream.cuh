@@ -25,14 +25,15 @@
 // plane g - LAG, for g = 0, 1, ...  A y-tile of plane z may load only after
 // all x-tiles of plane z are stored (a per-plane count, raised with release
 // semantics by each x-tile's producer once its store is complete, and read
-// with acquire semantics); by then the plane is
-// normally still in L2, so the field crosses HBM once in and once out.  The
-// count of an x-tile is raised one store later (when the next store is
-// issued, the previous one is complete or nearly so), so the producer rarely
-// waits for a store.  A producer whose next y-tile's plane is not ready only
+// with acquire semantics); by then the plane is normally still in L2, so the
+// field crosses HBM once in and once out.  The producer counts an x-tile as
+// soon as its store completes, after it has refilled the buffer (the compute
+// warps are busy with the other buffer meanwhile).  LAG (64 planes by
+// default: shorter lags leave y-tiles waiting, longer ones overflow L2) is
+// set per context.  A producer whose next y-tile's plane is not ready only
 // marks the buffer pending, and waits (bounded) for it when that buffer's
-// turn comes, after it has stored and counted every tile it holds with a
-// smaller ticket.  A waited-for x-tile therefore always has a smaller ticket
+// turn comes, when every tile it held with a smaller ticket is stored and
+// counted.  A waited-for x-tile therefore always has a smaller ticket
 // than the wait, and a CTA holding one either is not waiting or waits for a
 // still smaller ticket: no cycle, and the smallest waiting ticket's x-tiles
 // are all held by CTAs that finish them.  Every wait is bounded; one that
@@ -165,8 +166,11 @@ __global__ void __launch_bounds__(TSShape<T, N, RA, RB, P, RC>::THREADS, 2)
     cx<T>* land = reinterpret_cast<cx<T>*>(smem);  // [2] tiles
     cx<T>* xch = reinterpret_cast<cx<T>*>(smem + S_::OFF_XCH);
     float4* tws = reinterpret_cast<float4*>(smem + S_::OFF_TW);
+    // factor tables: V/2 along x and y (XY), or the K factor along z as
+    // (d.x, d.y, d.y, d.x) for the packed product (z pass)
     float2* d0_s = reinterpret_cast<float2*>(smem + S_::OFF_D);
     float2* d1_s = d0_s + N;
+    float4* dz_s = reinterpret_cast<float4*>(smem + S_::OFF_D);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + S_::OFF_BAR);
     uint64_t* done = full + 2;
     int4* slot = reinterpret_cast<int4*>(smem + S_::OFF_BAR + 32);  // [2] (kind, z, tile)
@@ -176,7 +180,8 @@ __global__ void __launch_bounds__(TSShape<T, N, RA, RB, P, RC>::THREADS, 2)
     L::build_stage_table(tws, reinterpret_cast<const float4*>(a.tw), tid, S_::THREADS);
     for (int i = tid; i < N; i += S_::THREADS) {
         if constexpr (KIND == TS_Z) {
-            d0_s[i] = a.kd[2][i];
+            const float2 d = a.kd[2][i];
+            dz_s[i] = make_float4(d.x, d.y, d.y, d.x);
         } else {
             d0_s[i] = a.vd[0][i];
             d1_s[i] = a.vd[1][i];
@@ -211,7 +216,6 @@ __global__ void __launch_bounds__(TSShape<T, N, RA, RB, P, RC>::THREADS, 2)
                 unsigned dpar, nfull;
             };
             Buf B0{0, 0, 0, 0, false, 0u, 0u}, B1{0, 0, 0, 0, false, 0u, 0u};
-            int unsig = -1;  // plane of an x-tile stored but not yet counted
             for (int i = 0; i < 8; ++i) s_ready[i] = 0u;
             auto known_ready = [&](int z) {
                 return z < 256 && ((s_ready[z >> 5] >> (z & 31)) & 1u);
@@ -226,11 +230,6 @@ __global__ void __launch_bounds__(TSShape<T, N, RA, RB, P, RC>::THREADS, 2)
                 // the store is complete: publish it to the y-tiles of plane z
                 asm volatile("fence.proxy.async.global;" ::: "memory");
                 red_release_add(k.done_x + z, 1);
-            };
-            auto flush = [&] {
-                asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
-                if (unsig >= 0) count(unsig);
-                unsig = -1;
             };
             auto map_of = [&](int kd) -> uint64_t {
                 return reinterpret_cast<uint64_t>(kd == TILE_Y ? &tm1 : &tm0);
@@ -290,8 +289,8 @@ __global__ void __launch_bounds__(TSShape<T, N, RA, RB, P, RC>::THREADS, 2)
                 constexpr int b = decltype(bc)::value;
                 if (m.tk >= total) return false;  // so is the other buffer's (a later ticket)
                 if (m.pend) {
-                    // everything held with a smaller ticket is stored and counted
-                    flush();
+                    // every tile held with a smaller ticket is stored and
+                    // counted (x-tiles are counted as their store completes)
                     unsigned polls = 0;
                     while (ld_acquire(k.done_x + m.z) < xi) {
                         if (++polls >= kPlaneWaitPolls) {
@@ -323,12 +322,12 @@ __global__ void __launch_bounds__(TSShape<T, N, RA, RB, P, RC>::THREADS, 2)
                 m.tk = (long)nxt;
                 prepare(bc, m);
                 if (m.tk < total) nxt = atomicAdd(k.ticket, 1ull);
-                if (unsig >= 0) {
-                    // the store before this one is complete
-                    asm volatile("cp.async.bulk.wait_group 1;" ::: "memory");
-                    count(unsig);
+                if (stored_x >= 0) {
+                    // the compute warps have the other buffer's tile: wait for
+                    // this store to complete and count it now
+                    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+                    count(stored_x);
                 }
-                unsig = stored_x;
                 return true;
             };
             using I0 = std::integral_constant<int, 0>;
@@ -340,7 +339,7 @@ __global__ void __launch_bounds__(TSShape<T, N, RA, RB, P, RC>::THREADS, 2)
             nxt = atomicAdd(k.ticket, 1ull);
             while (turn(I0{}, B0) && turn(I1{}, B1)) {
             }
-            flush();
+            asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
             if (!ok) {
                 // a wait gave up: let the loads still in flight land before
                 // the shared memory is released
@@ -415,7 +414,7 @@ __global__ void __launch_bounds__(TSShape<T, N, RA, RB, P, RC>::THREADS, 2)
                 const int x = tile * LT + l;  // z holds the y-row
                 L::template forward<true>(v, t, sl, twp, sync);
                 const cx<double> lf = cmul(ld2(a.kfac[0], x), ld2(a.kfac[1], z));
-                op_kphase_f32<L>(v, t, d0_s, line_delta(lf), (float)ks);
+                op_kphase_f32_packed<L>(v, t, dz_s, line_delta(lf), (float)ks);
 #pragma unroll
                 for (int e = 0; e < E; ++e) v[e].y = -v[e].y;
                 L::template forward<true>(v, t, sl, twp, sync);
