@@ -17,10 +17,10 @@ using namespace gpue_eng;
 namespace gpue_eng {
 
 std::vector<LPass> solve_passes(gpue_ctx* c, int i0, int i1, int gstate, bool guard,
-                                bool scale_step0) {
+                                bool scale_step0, bool plane) {
     std::vector<LPass> v;
     for (int i = i0; i < i1; ++i)
-        step_passes(c, i, gstate, gstate == 0 && (i > 0 || scale_step0), 1.0, guard, v);
+        step_passes(c, i, gstate, gstate == 0 && (i > 0 || scale_step0), 1.0, guard, v, plane);
     fuse(v);
     return v;
 }
@@ -79,23 +79,33 @@ bool mega_eligible(const gpue_ctx* c, int prec) {
     return true;
 }
 
+bool tile_eligible(const gpue_ctx* c, int prec) {
+    const char* env = std::getenv("GPUE_BATCH_TILE");
+    if (env && env[0] == '0') return false;
+    return prec == GPUE_PREC_FP32 && c->dim == 3 && !c->time_dep && c->N >= (1L << 20) &&
+           c->xy[prec].k && c->zpass[prec].k && plane_ok(c, prec);
+}
+
 void group_solves(BatchRun& r, int probe) {
     r.groups.clear();
     std::map<std::string, int> by_sig;
     for (size_t i = 0; i < r.ctx.size(); ++i) {
         gpue_ctx* c = r.ctx[i];
         const int off = r.offset[i];
+        const bool tile = tile_eligible(c, c->prec);
         const std::string sig =
-            std::to_string((int)r.guard[i]) + "/" +
+            std::to_string((int)r.guard[i]) + "/" + (tile ? "tile/" : "") +
             pass_signature(c, c->prec,
-                           solve_passes(c, off, off + probe, r.gstate, r.guard[i], r.scale_step0));
+                           solve_passes(c, off, off + probe, r.gstate, r.guard[i], r.scale_step0,
+                                        tile));
         auto it = by_sig.find(sig);
         if (it == by_sig.end()) {
             it = by_sig.emplace(sig, (int)r.groups.size()).first;
             BGroup g;
             g.prec = c->prec;
             g.guard = r.guard[i];
-            g.mega = mega_eligible(c, c->prec);
+            g.tile = tile;
+            g.mega = !tile && mega_eligible(c, c->prec);
             r.groups.push_back(g);
         }
         r.groups[it->second].members.push_back((int)i);
@@ -258,7 +268,7 @@ gpue_status plan_segment(const BatchRun& r, int s0, int s1, bool check, ArgSink&
             gpue_ctx* c = r.ctx[m];
             if (!g.mega)
                 lists[k] = solve_passes(c, r.offset[m] + s0, r.offset[m] + s1, r.gstate,
-                                        r.guard[m], r.scale_step0);
+                                        r.guard[m], r.scale_step0, g.tile);
             if (check)
                 for (const LPass& lp : energy_passes(c, r.gstate == 0)) lists[k].push_back(lp);
         }
@@ -278,6 +288,28 @@ gpue_status plan_segment(const BatchRun& r, int s0, int s1, bool check, ArgSink&
                     err = c->err;
                     return st;
                 }
+            }
+            // tile-stream passes: one launch per solve (its own tensor maps and
+            // counters); a converged solve's launch returns at once
+            TileLaunch tl0;
+            if (g.tile && tile_pass(c0, g.prec, lists[0][j], args[0], tl0)) {
+                for (int k = 0; k < n; ++k) {
+                    gpue_ctx* c = r.ctx[g.members[k]];
+                    TileLaunch tl;
+                    if (!tile_pass(c, g.prec, lists[k][j], args[k], tl)) {
+                        err = "batch group tile passes differ";
+                        return GPUE_ERR_STATE;
+                    }
+                    const PassArgs a = args[k];
+                    const bool pdl = j > 0 || k > 0;  // follows a pass kernel on this lane
+                    out_ops.push_back([=](cudaStream_t s) { launch_tile(tl, a, s, pdl); });
+                    sp.launches++;
+                }
+                continue;
+            }
+            if (axis >= kPlaneFwd) {
+                err = "batch group plane pass without a tile kernel";
+                return GPUE_ERR_STATE;
             }
             const LaunchCfg& lc = c0->lc[g.prec][axis];
             for (int k = 0; k < n; ++k) prefix[k] = (long)k * lc.ntiles;
@@ -665,7 +697,7 @@ gpue_status gpue_batch_evolve(gpue_batch* b, int32_t gstate, const gpue_batch_op
             k += "{" + std::to_string(g.guard) + "/" +
                  pass_signature(run.ctx[g.members[0]], g.prec,
                                 solve_passes(run.ctx[g.members[0]], 0, 3, gstate, g.guard,
-                                             false)) + "}";
+                                             false, g.tile)) + "}";
             for (int m : g.members) k += std::to_string(id[m]) + ",";
         }
         return k;

@@ -33,6 +33,7 @@ struct BGroup {
     int prec = 0;
     bool guard = false;
     bool mega = false;         // its solves run on the persistent multi-size kernel
+    bool tile = false;         // 3D complex64: the three tile-stream passes per step, per solve
     std::vector<int> members;  // indices into BatchRun::ctx
 };
 
@@ -61,8 +62,13 @@ struct SegPlan {
 
 // Passes of steps [i0, i1) of one solve (imaginary-time steps after the
 // first renormalise; step 0 too when scale_step0).
+// plane: the 3D complex64 schedule of the tile-stream (or plane) passes.
 std::vector<LPass> solve_passes(gpue_ctx* c, int i0, int i1, int gstate, bool guard,
-                                bool scale_step0);
+                                bool scale_step0, bool plane = false);
+// Whether a solve's steps run as the tile-stream passes in a batch: 3D
+// complex64 with the XY and z tile kernels planned, at least 2^20 points
+// (smaller grids do better sharing launches), GPUE_BATCH_TILE not 0.
+bool tile_eligible(const gpue_ctx* c, int prec);
 // Launch-relevant description of a pass list: equal strings can share launches.
 std::string pass_signature(const gpue_ctx* c, int prec, const std::vector<LPass>& v);
 // Groups r.ctx by the signature of steps [0, probe) from each solve's offset.

@@ -552,27 +552,58 @@ gpue_status make_pass_args(gpue_ctx* c, int prec, const LPass& lp, int gstate, P
 }
 
 // pdl: the previous operation in the stream is a pass kernel
+bool tile_pass(gpue_ctx* c, int prec, const LPass& lp, const PassArgs& a, TileLaunch& t) {
+    if (lp.axis >= kPlaneFwd && c->xy[prec].k) {
+        const XYCfg& xc = c->xy[prec];
+        t.fn = lp.axis == kPlaneFwd ? xc.k->fwd : xc.k->inv;
+        t.tm0 = &xc.tmx;
+        t.tm1 = &xc.tmy;
+        t.kc = xc.ctr.dev();
+        t.blocks = xc.blocks;
+        t.threads = xc.k->threads;
+        t.smem = xc.k->smem;
+        return true;
+    }
+    const ZCfg& zc = c->zpass[prec];
+    if (lp.axis == 2 && zc.k && !c->ext && lp.red == RED_NONE && lp.store &&
+        !lp.from_scratch && !lp.to_scratch && a.in == state_of(c, prec) &&
+        lp.ops == std::vector<int>{OP_FFT_F, OP_KPHASE, OP_FFT_I}) {
+        t.fn = zc.k->fn;
+        t.tm0 = t.tm1 = &zc.tm;
+        t.kc = zc.ctr.dev();
+        t.blocks = zc.blocks;
+        t.threads = zc.k->threads;
+        t.smem = zc.k->smem;
+        return true;
+    }
+    return false;
+}
+
+cudaError_t launch_tile(const TileLaunch& t, const PassArgs& a, cudaStream_t s, bool pdl) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(t.blocks);
+    cfg.blockDim = dim3(t.threads);
+    cfg.dynamicSmemBytes = t.smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    PassArgs pa = a;
+    XYCounters kc = t.kc;
+    void* args[] = {const_cast<CUtensorMap*>(t.tm0), const_cast<CUtensorMap*>(t.tm1), &pa, &kc};
+    return cudaLaunchKernelExC(&cfg, t.fn, args);
+}
+
 gpue_status launch_pass(gpue_ctx* c, int prec, const LPass& lp, int gstate, bool pdl) {
     PassArgs a;
     gpue_status st = make_pass_args(c, prec, lp, gstate, a);
     if (st) return st;
     a.active = nullptr;  // a single solve always runs
-    if (lp.axis >= kPlaneFwd && c->xy[prec].k) {
-        const XYCfg& xc = c->xy[prec];
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(xc.blocks);
-        cfg.blockDim = dim3(xc.k->threads);
-        cfg.dynamicSmemBytes = xc.k->smem;
-        cfg.stream = c->stream;
-        cudaLaunchAttribute at[1];
-        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        at[0].val.programmaticStreamSerializationAllowed = 1;
-        cfg.attrs = at;
-        cfg.numAttrs = pdl ? 1 : 0;
-        XYCounters kc = xc.ctr.dev();
-        void* args[] = {const_cast<CUtensorMap*>(&xc.tmx), const_cast<CUtensorMap*>(&xc.tmy),
-                        &a, &kc};
-        CK(cudaLaunchKernelExC(&cfg, lp.axis == kPlaneFwd ? xc.k->fwd : xc.k->inv, args));
+    TileLaunch tl;
+    if (tile_pass(c, prec, lp, a, tl)) {
+        CK(launch_tile(tl, a, c->stream, pdl));
         c->launches++;
         return GPUE_OK;
     }
@@ -593,27 +624,6 @@ gpue_status launch_pass(gpue_ctx* c, int prec, const LPass& lp, int gstate, bool
         cfg.attrs = at;
         cfg.numAttrs = pdl ? 2 : 1;
         CK(cudaLaunchKernelEx(&cfg, lp.axis == kPlaneFwd ? pc.k->fwd : pc.k->inv, a));
-        c->launches++;
-        return GPUE_OK;
-    }
-    const ZCfg& zc = c->zpass[prec];
-    if (lp.axis == 2 && zc.k && !c->ext && lp.red == RED_NONE && lp.store &&
-        !lp.from_scratch && !lp.to_scratch && a.in == state_of(c, prec) &&
-        lp.ops == std::vector<int>{OP_FFT_F, OP_KPHASE, OP_FFT_I}) {
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(zc.blocks);
-        cfg.blockDim = dim3(zc.k->threads);
-        cfg.dynamicSmemBytes = zc.k->smem;
-        cfg.stream = c->stream;
-        cudaLaunchAttribute at[1];
-        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        at[0].val.programmaticStreamSerializationAllowed = 1;
-        cfg.attrs = at;
-        cfg.numAttrs = pdl ? 1 : 0;
-        XYCounters kc = zc.ctr.dev();
-        void* args[] = {const_cast<CUtensorMap*>(&zc.tm), const_cast<CUtensorMap*>(&zc.tm), &a,
-                        &kc};
-        CK(cudaLaunchKernelExC(&cfg, zc.k->fn, args));
         c->launches++;
         return GPUE_OK;
     }

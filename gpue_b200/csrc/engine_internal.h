@@ -249,6 +249,20 @@ gpue_status plan_axis(gpue_ctx* c, int prec, int axis);
 // and keeps the fastest for each axis (cached per shape for the process).
 gpue_status autotune_ctx(gpue_ctx* c, int prec, bool force);
 gpue_status make_pass_args(gpue_ctx* c, int prec, const LPass& lp, int gstate, PassArgs& a);
+// A tile-stream launch (tstream.cuh): the kernel, the context's tensor maps
+// (they live as long as the context), the work counters and the grid.
+struct TileLaunch {
+    const void* fn = nullptr;
+    const CUtensorMap* tm0 = nullptr;
+    const CUtensorMap* tm1 = nullptr;
+    XYCounters kc{};
+    int blocks = 0, threads = 0;
+    size_t smem = 0;
+};
+// Whether pass lp of c runs as a tile-stream kernel (the XY passes, and the
+// in-place F K I z pass, where planned), and that launch.
+bool tile_pass(gpue_ctx* c, int prec, const LPass& lp, const PassArgs& a, TileLaunch& t);
+cudaError_t launch_tile(const TileLaunch& t, const PassArgs& a, cudaStream_t s, bool pdl);
 // plane: run the in-plane axes of a 3D step as the two XY-plane passes
 void step_passes(gpue_ctx* c, int i, int gstate, bool scale_first, double rexp, int guard,
                  std::vector<LPass>& out, bool plane = false);

@@ -195,6 +195,13 @@ __global__ void __launch_bounds__(TSShape<T, N, RA, RB, P, RC>::THREADS, 2)
     }
     __syncthreads();
     pdl_wait();  // the field and the scale are the previous kernel's output
+    // a converged solve of a batched run (its active flag cleared by the
+    // previous check) is left as it is: every CTA returns before touching the
+    // field or the work counters
+    if (a.active && *reinterpret_cast<const volatile int*>(a.active) == 0) {
+        pdl_launch_dependents();
+        return;
+    }
 
     const int nz = a.nz;
     const int xi = a.ny / LT, yi = a.nx / LT;  // x-tiles (and y- or z-tiles) per plane
