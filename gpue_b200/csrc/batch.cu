@@ -82,7 +82,9 @@ bool mega_eligible(const gpue_ctx* c, int prec) {
 bool tile_eligible(const gpue_ctx* c, int prec) {
     const char* env = std::getenv("GPUE_BATCH_TILE");
     if (env && env[0] == '0') return false;
-    return prec == GPUE_PREC_FP32 && c->dim == 3 && !c->time_dep && c->N >= (1L << 20) &&
+    long min_points = 1L << 20;
+    if (const char* m = std::getenv("GPUE_BATCH_TILE_MIN")) min_points = std::atol(m);
+    return prec == GPUE_PREC_FP32 && c->dim == 3 && !c->time_dep && c->N >= min_points &&
            c->xy[prec].k && c->zpass[prec].k && plane_ok(c, prec);
 }
 

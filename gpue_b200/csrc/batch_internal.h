@@ -66,8 +66,9 @@ struct SegPlan {
 std::vector<LPass> solve_passes(gpue_ctx* c, int i0, int i1, int gstate, bool guard,
                                 bool scale_step0, bool plane = false);
 // Whether a solve's steps run as the tile-stream passes in a batch: 3D
-// complex64 with the XY and z tile kernels planned, at least 2^20 points
-// (smaller grids do better sharing launches), GPUE_BATCH_TILE not 0.
+// complex64 with the XY and z tile kernels planned, at least
+// GPUE_BATCH_TILE_MIN points (default 2^20: smaller grids do better sharing
+// launches), GPUE_BATCH_TILE not 0.
 bool tile_eligible(const gpue_ctx* c, int prec);
 // Launch-relevant description of a pass list: equal strings can share launches.
 std::string pass_signature(const gpue_ctx* c, int prec, const std::vector<LPass>& v);
