@@ -24,7 +24,9 @@
 // Transforms are unnormalised with cuFFT's signs (forward exp(-2 pi i jk/N)),
 // which is what GPUE's evolve() uses before its 1/sqrt(N) scalarMult; the
 // passes fold the 1/N of each forward/inverse pair into a phase factor.  The
-// inverse is conj(F(conj(x))), so one FFT body serves both directions.
+// inverse is conj(F(conj(x))): either conjugated around the forward body, or
+// the same body with every twiddle and +-i conjugated (forward<.., true>),
+// which gives the same values without the conjugation sweeps.
 
 #pragma once
 
@@ -55,9 +57,11 @@ template <typename T>
 __device__ __forceinline__ cx<T> cscale(cx<T> a, T s) { return {a.x * s, a.y * s}; }
 template <typename T>
 __device__ __forceinline__ cx<T> cconj(cx<T> a) { return {a.x, -a.y}; }
-// multiply by -i
+// multiply by -i, by +i
 template <typename T>
 __device__ __forceinline__ cx<T> mul_mi(cx<T> a) { return {a.y, -a.x}; }
+template <typename T>
+__device__ __forceinline__ cx<T> mul_pi(cx<T> a) { return {-a.y, a.x}; }
 
 // Complex64 sums and differences as packed FP32x2 operations (sm_100: one
 // instruction for both components).  Each component is rounded exactly as
@@ -86,6 +90,13 @@ __device__ __forceinline__ cx<float> cmul_split(cx<float> a, cx<float> hi, cx<fl
     const float tx = fmaf(a.x, lo.x, -a.y * lo.y);
     const float ty = fmaf(a.x, lo.y, a.y * lo.x);
     return {fmaf(a.x, hi.x, fmaf(-a.y, hi.y, tx)), fmaf(a.x, hi.y, fmaf(a.y, hi.x, ty))};
+}
+// a * conj(hi + lo), the product cmul_split forms on conjugated values,
+// conjugated (the same operations with the signs moved: bit-identical)
+__device__ __forceinline__ cx<float> cmul_split_conj(cx<float> a, cx<float> hi, cx<float> lo) {
+    const float tx = fmaf(a.x, lo.x, a.y * lo.y);
+    const float ty = fmaf(-a.x, lo.y, a.y * lo.x);
+    return {fmaf(a.x, hi.x, fmaf(a.y, hi.y, tx)), fmaf(-a.x, hi.y, fmaf(a.y, hi.x, ty))};
 }
 // The same product for a constant twiddle, as four packed FP32x2 operations
 // in the same order (bit-identical to cmul_split): the constant pairs
@@ -131,13 +142,16 @@ __device__ __forceinline__ cx<T> tw_const(cx<T> a) {
 }
 
 // ---------------------------------------------------------- small DFTs --
-// In-place forward R-point DFT of v[0..R-1] in registers, natural order.
+// In-place R-point DFT of v[0..R-1] in registers, natural order: forward
+// (exp(-2 pi i jk/R)), or with INV the inverse (exp(+2 pi i jk/R)), which
+// equals conj(F(conj v)) operation for operation (every twiddle and +-i
+// conjugated), so no conjugation pass is needed around it.
 
-template <int R, typename T>
+template <int R, typename T, bool INV = false>
 struct SmallDFT;
 
-template <typename T>
-struct SmallDFT<2, T> {
+template <typename T, bool INV>
+struct SmallDFT<2, T, INV> {
     static __device__ __forceinline__ void run(cx<T>* v) {
         cx<T> a = v[0], b = v[1];
         v[0] = a + b;
@@ -145,26 +159,29 @@ struct SmallDFT<2, T> {
     }
 };
 
-template <typename T>
-struct SmallDFT<3, T> {
+template <typename T, bool INV>
+struct SmallDFT<3, T, INV> {
     static __device__ __forceinline__ void run(cx<T>* v) {
         constexpr T c1 = (T)-0.5;
         constexpr T s1 = (T)-tw_sin(3, 1);
         cx<T> t1 = v[1] + v[2];
         cx<T> t2 = v[1] - v[2];
         cx<T> a = {v[0].x + c1 * t1.x, v[0].y + c1 * t1.y};
-        cx<T> b = {-s1 * t2.y, s1 * t2.x};  // i*s1*t2
+        cx<T> b;  // i*s1*t2 (forward), -i*s1*t2 (inverse)
+        if constexpr (INV) b = {s1 * t2.y, -s1 * t2.x};
+        else b = {-s1 * t2.y, s1 * t2.x};
         v[0] = v[0] + t1;
         v[1] = a + b;
         v[2] = a - b;
     }
 };
 
-template <typename T>
-struct SmallDFT<4, T> {
+template <typename T, bool INV>
+struct SmallDFT<4, T, INV> {
     static __device__ __forceinline__ void run(cx<T>* v) {
         cx<T> s02 = v[0] + v[2], d02 = v[0] - v[2];
-        cx<T> s13 = v[1] + v[3], d13 = mul_mi(v[1] - v[3]);
+        cx<T> s13 = v[1] + v[3];
+        cx<T> d13 = INV ? mul_pi(v[1] - v[3]) : mul_mi(v[1] - v[3]);
         v[0] = s02 + s13;
         v[1] = d02 + d13;
         v[2] = s02 - s13;
@@ -172,22 +189,27 @@ struct SmallDFT<4, T> {
     }
 };
 
-// Complex64: the four sums and differences packed, the -i products as scalar
-// component sums (the same values as the generic form)
-template <>
-struct SmallDFT<4, float> {
+// Complex64: the four sums and differences packed, the +-i products as
+// scalar component sums (the same values as the generic form)
+template <bool INV>
+struct SmallDFT<4, float, INV> {
     static __device__ __forceinline__ void run(cx<float>* v) {
         const cx<float> s02 = v[0] + v[2], d02 = v[0] - v[2];
         const cx<float> s13 = v[1] + v[3], d13 = v[1] - v[3];
         v[0] = s02 + s13;
         v[2] = s02 - s13;
-        v[1] = {d02.x + d13.y, d02.y - d13.x};
-        v[3] = {d02.x - d13.y, d02.y + d13.x};
+        if constexpr (INV) {
+            v[1] = {d02.x - d13.y, d02.y + d13.x};
+            v[3] = {d02.x + d13.y, d02.y - d13.x};
+        } else {
+            v[1] = {d02.x + d13.y, d02.y - d13.x};
+            v[3] = {d02.x - d13.y, d02.y + d13.x};
+        }
     }
 };
 
-template <typename T>
-struct SmallDFT<5, T> {
+template <typename T, bool INV>
+struct SmallDFT<5, T, INV> {
     static __device__ __forceinline__ void run(cx<T>* v) {
         constexpr T c1 = (T)tw_cos(5, 1), c2 = (T)tw_cos(5, 2);
         constexpr T s1 = (T)-tw_sin(5, 1);
@@ -196,9 +218,15 @@ struct SmallDFT<5, T> {
         cx<T> a2 = v[2] + v[3], b2 = v[2] - v[3];
         cx<T> r1 = {v[0].x + c1 * a1.x + c2 * a2.x, v[0].y + c1 * a1.y + c2 * a2.y};
         cx<T> r2 = {v[0].x + c2 * a1.x + c1 * a2.x, v[0].y + c2 * a1.y + c1 * a2.y};
-        // i*(s1 b1 + s2 b2) and i*(s2 b1 - s1 b2)
-        cx<T> i1 = {-(s1 * b1.y + s2 * b2.y), s1 * b1.x + s2 * b2.x};
-        cx<T> i2 = {-(s2 * b1.y - s1 * b2.y), s2 * b1.x - s1 * b2.x};
+        // i*(s1 b1 + s2 b2) and i*(s2 b1 - s1 b2); -i times the same (inverse)
+        cx<T> i1, i2;
+        if constexpr (INV) {
+            i1 = {s1 * b1.y + s2 * b2.y, -(s1 * b1.x + s2 * b2.x)};
+            i2 = {s2 * b1.y - s1 * b2.y, -(s2 * b1.x - s1 * b2.x)};
+        } else {
+            i1 = {-(s1 * b1.y + s2 * b2.y), s1 * b1.x + s2 * b2.x};
+            i2 = {-(s2 * b1.y - s1 * b2.y), s2 * b1.x - s1 * b2.x};
+        }
         v[0] = v[0] + a1 + a2;
         v[1] = r1 + i1;
         v[4] = r1 - i1;
@@ -208,7 +236,8 @@ struct SmallDFT<5, T> {
 };
 
 // Composite R = A*B: B DFTs of length A on stride-B subsequences, twiddles
-// W_R^{b k1}, then A DFTs of length B; X[k1 + A*k2].
+// W_R^{b k1} (conjugated for the inverse), then A DFTs of length B;
+// X[k1 + A*k2].
 template <int R>
 struct Split {
     static constexpr int A = (R % 4 == 0 && R != 8 && R != 4) ? 4
@@ -218,13 +247,13 @@ struct Split {
     static constexpr int B = R / A;
 };
 
-template <int R, typename T>
+template <int R, typename T, bool INV>
 struct SmallDFT {
     static constexpr int A = Split<R>::A;
     static constexpr int B = Split<R>::B;
     template <int b, int k1>
     static __device__ __forceinline__ void tw_one(cx<T> (&y)[B][A]) {
-        y[b][k1] = tw_const<R, b * k1>(y[b][k1]);
+        y[b][k1] = tw_const<R, INV ? -(b * k1) : b * k1>(y[b][k1]);
     }
     template <int... I>
     static __device__ __forceinline__ void twiddle_all(cx<T> (&y)[B][A],
@@ -237,7 +266,7 @@ struct SmallDFT {
         for (int b = 0; b < B; ++b) {
 #pragma unroll
             for (int a = 0; a < A; ++a) y[b][a] = v[b + B * a];
-            SmallDFT<A, T>::run(y[b]);
+            SmallDFT<A, T, INV>::run(y[b]);
         }
         twiddle_all(y, std::make_integer_sequence<int, B * A>{});
         cx<T> z[B];
@@ -245,7 +274,7 @@ struct SmallDFT {
         for (int k1 = 0; k1 < A; ++k1) {
 #pragma unroll
             for (int b = 0; b < B; ++b) z[b] = y[b][k1];
-            SmallDFT<B, T>::run(z);
+            SmallDFT<B, T, INV>::run(z);
 #pragma unroll
             for (int k2 = 0; k2 < B; ++k2) v[k1 + A * k2] = z[k2];
         }
@@ -369,25 +398,36 @@ struct LineFFT {
                 }
             }
         }
+        // a times the twiddle (INV: its conjugate)
+        template <bool INV>
+        __device__ __forceinline__ cx<T> twmul(cx<T> a, cx<T> hi, cx<T> lo) const {
+            if constexpr (SPLIT) {
+                if constexpr (INV) return cmul_split_conj(a, hi, lo);
+                else return cmul_split(a, hi, lo);
+            } else {
+                return cmul(a, INV ? cconj(hi) : hi);
+            }
+        }
+        template <bool INV = false>
         __device__ __forceinline__ cx<T> mul(cx<T> a, int q, int r) const {
             if constexpr (HOLD) {
                 const int qq = NQ == 1 ? 0 : q;
-                if constexpr (SPLIT) return cmul_split(a, w[qq][r - 1][0], w[qq][r - 1][1]);
-                else return cmul(a, w[qq][r - 1][0]);
+                return twmul<INV>(a, w[qq][r - 1][0], w[qq][r - 1][WPER - 1]);
             } else {
                 const int k = TWS ? tw_index<S>((t + P * q) % Ns, r)
                                   : ((t + P * q) % Ns) * r * step;
                 if constexpr (SPLIT) {
                     const float4 e = tw4<TWS>(reinterpret_cast<const float4*>(tw) + k);
-                    return cmul_split(a, cx<float>{e.x, e.y}, cx<float>{e.z, e.w});
+                    return twmul<INV>(a, cx<T>{e.x, e.y}, cx<T>{e.z, e.w});
                 } else {
-                    return cmul(a, tw1<TWS>(tw + k));
+                    const cx<T> e = tw1<TWS>(tw + k);
+                    return twmul<INV>(a, e, e);
                 }
             }
         }
     };
 
-    template <int S, bool TWS = false>
+    template <int S, bool TWS = false, bool INV = false>
     static __device__ __forceinline__ void compute(cx<T> (&v)[E], const StageTw<S, TWS>* w) {
         constexpr int R = radix(S);
         constexpr int G = N / (R * P);
@@ -395,9 +435,10 @@ struct LineFFT {
         for (int q = 0; q < G; ++q) {
             if constexpr (S > 0) {
 #pragma unroll
-                for (int r = 1; r < R; ++r) v[q * R + r] = w->mul(v[q * R + r], q, r);
+                for (int r = 1; r < R; ++r)
+                    v[q * R + r] = w->template mul<INV>(v[q * R + r], q, r);
             }
-            SmallDFT<R, T>::run(&v[q * R]);
+            SmallDFT<R, T, INV>::run(&v[q * R]);
         }
     }
 
@@ -428,25 +469,26 @@ struct LineFFT {
 
     // One stage after the first: its twiddles are requested before the
     // exchange, so their latency overlaps the shared-memory round trip.
-    template <int S, bool TWS, typename Sync>
+    template <int S, bool TWS, bool INV, typename Sync>
     static __device__ __forceinline__ void stage(cx<T> (&v)[E], int t, cx<T>* sl,
                                                  const cx<T>* __restrict__ tw, Sync sync) {
         StageTw<S, TWS> w;
         w.load(t, tw);
         exchange<S - 1>(v, t, sl, sync);
-        compute<S, TWS>(v, &w);
+        compute<S, TWS, INV>(v, &w);
     }
 
-    // Unnormalised forward DFT of the line (inverse: conjugate around it).
-    // TWS: tw points to the per-stage table (build_stage_table) in shared
-    // memory.
-    template <bool TWS = false, typename Sync>
+    // Unnormalised DFT of the line: forward, or with INV the inverse with
+    // conjugated twiddles (the same values as conjugating around the
+    // forward transform, without the two conjugation sweeps).  TWS: tw points
+    // to the per-stage table (build_stage_table) in shared memory.
+    template <bool TWS = false, bool INV = false, typename Sync>
     static __device__ __forceinline__ void forward(cx<T> (&v)[E], int t, cx<T>* sl,
                                                    const cx<T>* __restrict__ tw, Sync sync) {
-        compute<0, TWS>(v, static_cast<const StageTw<0, TWS>*>(nullptr));
-        stage<1, TWS>(v, t, sl, tw, sync);
-        if constexpr (NS >= 3) stage<2, TWS>(v, t, sl, tw, sync);
-        if constexpr (NS >= 4) stage<3, TWS>(v, t, sl, tw, sync);
+        compute<0, TWS, INV>(v, static_cast<const StageTw<0, TWS>*>(nullptr));
+        stage<1, TWS, INV>(v, t, sl, tw, sync);
+        if constexpr (NS >= 3) stage<2, TWS, INV>(v, t, sl, tw, sync);
+        if constexpr (NS >= 4) stage<3, TWS, INV>(v, t, sl, tw, sync);
     }
 };
 

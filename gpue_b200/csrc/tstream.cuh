@@ -406,11 +406,7 @@ __global__ void __launch_bounds__(TSShape<T, N, RA, RB, P, RC>::THREADS, 2)
                 }
                 L::template forward<true>(v, t, sl, twp, sync);
             } else if constexpr (KIND == TS_XY_INV) {
-#pragma unroll
-                for (int e = 0; e < E; ++e) v[e].y = -v[e].y;
-                L::template forward<true>(v, t, sl, twp, sync);
-#pragma unroll
-                for (int e = 0; e < E; ++e) v[e].y = -v[e].y;
+                L::template forward<true, true>(v, t, sl, twp, sync);  // inverse
                 if (!rows) {
                     const int x = tile * LT + l;
                     const cx<double> lf = cmul(ld2(a.vfac[0], x), ld2(a.vfac[2], z));
@@ -422,11 +418,7 @@ __global__ void __launch_bounds__(TSShape<T, N, RA, RB, P, RC>::THREADS, 2)
                 L::template forward<true>(v, t, sl, twp, sync);
                 const cx<double> lf = cmul(ld2(a.kfac[0], x), ld2(a.kfac[1], z));
                 op_kphase_f32_packed<L>(v, t, dz_s, line_delta(lf), (float)ks);
-#pragma unroll
-                for (int e = 0; e < E; ++e) v[e].y = -v[e].y;
-                L::template forward<true>(v, t, sl, twp, sync);
-#pragma unroll
-                for (int e = 0; e < E; ++e) v[e].y = -v[e].y;
+                L::template forward<true, true>(v, t, sl, twp, sync);  // inverse
             }
             if (rows) {
 #pragma unroll
