@@ -858,7 +858,8 @@ def main():
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get("head_fp32_dominant_pass_bytes_per_launch")
+            per_kind = json.load(open(tpath)).get("head_fp32_pass_bytes_per_launch", {})
+            traffic = per_kind.get({3: "forward_xy", 2: "z", 4: "inverse_xy"}.get(dom_kind))
         except Exception:
             traffic = None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
