@@ -583,6 +583,8 @@ def serve_leg(G, dev):
             "sequential_wall_s": seq_wall,
             "served_over_sequential": (ok / wall) / (len(reqs) / seq_wall),
             "device_busy_s": stats["busy_s"], "ticks": stats["ticks"],
+            "worker_host_s": {"admit": stats["admit_s"], "issue": stats["issue_s"],
+                              "finish": stats["finish_s"]},
             "admitted_in_tick": stats["admitted_in_tick"],
             "kernel_launches": stats["kernel_launches"],
             "point_steps_per_s": stats["point_steps"] / wall,

@@ -10,6 +10,10 @@
 // reached max_steps leave after the tick: their state is written to the
 // caller's buffer, their context freed and their result queued for polling.
 //
+// The solves that leave at a tick return their results while the next tick
+// runs (their copies use their own streams), and their contexts are freed at
+// the following idle point, so the device does not wait for the copy-outs.
+//
 // Deadlines and cancellation are host-side: a request whose deadline has
 // passed, or whose tag was cancelled, leaves the queue at once, or leaves the
 // resident set after the tick in flight with its state at that tick; nothing
@@ -138,6 +142,15 @@ struct Pending {
     double t_submit;
 };
 
+// A solve that left the resident set at a tick: its result is written out
+// while the next tick runs.
+struct Leaving {
+    Solve s;
+    BatchOut bo;
+    bool stopped;
+    gpue_status why;
+};
+
 }  // namespace
 
 struct gpue_server {
@@ -155,6 +168,8 @@ struct gpue_server {
     bool broken = false;                   // guarded by mu
     std::string err;                       // guarded by mu
     std::vector<Solve> active;             // worker only
+    std::vector<Leaving> leaving;          // worker only: left at the last tick
+    std::vector<Solve> zombies;            // worker only: results out, contexts to free
     Run run[2];                            // worker only
     uint64_t next_serial = 1;              // worker only
 };
@@ -408,11 +423,12 @@ gpue_status issue_run(gpue_server* S, int gstate, Run& R, long& launches, std::s
     return GPUE_OK;
 }
 
-// Finishes a solve: final scaling, copy-out, result, context freed.  `why`
-// is GPUE_OK for a solve that ran to its end, or the timeout / cancellation
-// status of one that leaves early (its state still goes to psi_out).
-void finish(gpue_server* S, Solve& s, const BatchOut& bo, bool stopped,
-            gpue_status why = GPUE_OK) {
+// A solve's result: final scaling, copy-out, result (to push).  `why` is
+// GPUE_OK for a solve that ran to its end, or the timeout / cancellation
+// status of one that leaves early (its state still goes to psi_out).  Its
+// context stays allocated (and counted against the budget) until release().
+gpue_server_result finish(gpue_server* S, Solve& s, const BatchOut& bo, bool stopped,
+                          gpue_status why = GPUE_OK) {
     gpue_ctx* c = s.c;
     gpue_status st = GPUE_OK;
     if (s.req.gstate == 0) c->pending_scale = true;
@@ -424,18 +440,53 @@ void finish(gpue_server* S, Solve& s, const BatchOut& bo, bool stopped,
     r.steps_done = stopped ? bo.steps : s.steps;
     r.early_stop = stopped ? 1 : 0;
     r.energy = bo.checks > 0 ? bo.energy : NAN;
-    gpue_ctx_destroy(c);
-    s.c = nullptr;
     {
         std::lock_guard<std::mutex> lk(S->mu);
-        S->st.bytes_resident -= (int64_t)s.bytes;
-        S->st.active--;
         if (r.status == GPUE_ERR_TIMEOUT) S->st.timed_out++;
         if (r.status == GPUE_ERR_CANCELLED) S->st.cancelled++;
         auto it = S->resident_tags.find(s.req.tag);
         if (it != S->resident_tags.end()) S->resident_tags.erase(it);
     }
-    push_result(S, r);
+    return r;
+}
+
+// Frees a finished solve's context (cudaFree waits for the device, so this
+// runs where the device is idle anyway) and its share of the budget.
+void release(gpue_server* S, Solve& s) {
+    if (s.c) gpue_ctx_destroy(s.c);
+    s.c = nullptr;
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->st.bytes_resident -= (int64_t)s.bytes;
+    S->st.active--;
+}
+
+// The results of the solves that left at the last tick, while the next one
+// runs (their copies use their own streams); their contexts wait for
+// release_zombies.  With release_now (no tick follows) each context is
+// freed before its result goes out.
+void finish_leaving(gpue_server* S, bool release_now) {
+    if (S->leaving.empty()) return;
+    const auto tf = std::chrono::steady_clock::now();
+    for (Leaving& l : S->leaving) {
+        const gpue_server_result r = finish(S, l.s, l.bo, l.stopped, l.why);
+        if (release_now) release(S, l.s);
+        else S->zombies.push_back(l.s);
+        push_result(S, r);
+    }
+    S->leaving.clear();
+    const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - tf).count();
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->st.finish_s += dt;
+}
+
+void release_zombies(gpue_server* S) {
+    if (S->zombies.empty()) return;
+    const auto tf = std::chrono::steady_clock::now();
+    for (Solve& s : S->zombies) release(S, s);
+    S->zombies.clear();
+    const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - tf).count();
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->st.finish_s += dt;
 }
 
 // Enqueues one tick of every resident solve (both runs); returns without
@@ -474,6 +525,8 @@ gpue_status tick_complete(gpue_server* S, long launches, std::string& err) {
         cudaEventElapsedTime(&ms, first->e0, R.e1);
         busy = std::max(busy, (double)ms * 1e-3);
     }
+    // the device is idle: free the contexts whose results went out meanwhile
+    release_zombies(S);
     std::vector<char> leave(S->active.size(), 0);
     const auto tf = std::chrono::steady_clock::now();
     std::set<int64_t> cancel;
@@ -497,9 +550,10 @@ gpue_status tick_complete(gpue_server* S, long launches, std::string& err) {
                 else if (expired(s.req, s.t_submit, now)) why = GPUE_ERR_TIMEOUT;
             }
             if (stopped || s.steps >= s.req.max_steps || why != GPUE_OK) {
-                finish(S, s, bo, stopped, why);
+                // its result goes out while the next tick runs
+                S->leaving.push_back(Leaving{s, bo, stopped, why});
                 leave[R.members[k]] = 1;
-                R.drop_graph();  // its arguments name the context just freed
+                R.drop_graph();  // its arguments name a context leaving the run
             }
         }
     }
@@ -530,7 +584,8 @@ void worker_main(gpue_server* S) {
     for (;;) {
         {
             std::unique_lock<std::mutex> lk(S->mu);
-            if (S->active.empty() && S->queue.empty())
+            if (S->active.empty() && S->queue.empty() && S->leaving.empty() &&
+                S->zombies.empty())
                 S->cv_work.wait_for(lk, std::chrono::milliseconds(20),
                                     [&] { return S->stop || !S->queue.empty(); });
             if (S->stop) return;
@@ -545,10 +600,16 @@ void worker_main(gpue_server* S) {
         };
         drop_expired(S);
         timed_admit(true);
-        if (S->active.empty()) continue;
+        if (S->active.empty()) {
+            // no tick to overlap: free the last leavers and return them now
+            release_zombies(S);
+            finish_leaving(S, true);
+            continue;
+        }
         std::string err;
         long launches = 0;
         gpue_status st = tick_issue(S, launches, err);
+        if (!st) finish_leaving(S, false);
         // requests that arrive while the device runs the tick are set up
         // meanwhile (they join the next tick)
         while (!st) {
@@ -567,6 +628,8 @@ void worker_main(gpue_server* S) {
             // the device state of every resident solve is now unknown; let
             // whatever was enqueued drain before the contexts are freed
             cudaDeviceSynchronize();
+            release_zombies(S);
+            finish_leaving(S, true);
             for (Solve& s : S->active) {
                 push_result(S, make_result(s.req, st, s.t_submit, s.t_admit, now_s(S)));
                 gpue_ctx_destroy(s.c);
@@ -642,6 +705,10 @@ gpue_status gpue_server_destroy(gpue_server* S) {
     if (S->worker.joinable()) S->worker.join();
     cudaSetDevice(S->o.device);
     for (Solve& s : S->active)
+        if (s.c) gpue_ctx_destroy(s.c);
+    for (Leaving& l : S->leaving)
+        if (l.s.c) gpue_ctx_destroy(l.s.c);
+    for (Solve& s : S->zombies)
         if (s.c) gpue_ctx_destroy(s.c);
     for (Run& R : S->run) {
         if (R.stream) cudaStreamSynchronize(R.stream);
