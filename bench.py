@@ -609,10 +609,12 @@ def cpu_oracle_rate(psi0, budget_s=15.0, threads=0):
     n = HEAD["n"]
     P = oracle.Problem(3, n, HEAD["box"], wz=HEAD["wz"], g=HEAD["g"], gdt=HEAD["gdt"],
                        threads=threads)
+    psi, _, _ = P.evolve(psi0, 1, 0)  # warm-up (first-call set-up)
     t = time.time()
-    psi, _, _ = P.evolve(psi0, 1, 0)
-    per = time.time() - t
-    steps = max(1, min(50, int(budget_s / max(per, 1e-6))))
+    psi, _, _ = P.evolve(psi, 2, 0)
+    per = (time.time() - t) / 2
+    # a sample of about budget_s seconds
+    steps = max(1, min(100, int(budget_s / max(per, 1e-6))))
     t = time.time()
     P.evolve(psi, steps, 0)
     dt = time.time() - t
