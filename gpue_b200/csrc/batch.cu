@@ -141,12 +141,12 @@ gpue_status plan_mega(const BatchRun& r, int prec, int s0, int s1, ArgSink& sink
     if (solves.empty()) return GPUE_OK;
     const int ns = (int)solves.size();
     std::vector<std::vector<LPass>> lists(ns);
-    size_t rounds = 0;
+    size_t depth = 0;  // the longest pass list
     for (int k = 0; k < ns; ++k) {
         const int m = solves[k];
         lists[k] = solve_passes(r.ctx[m], r.offset[m] + s0, r.offset[m] + s1, r.gstate,
                                 r.guard[m], r.scale_step0);
-        rounds = std::max(rounds, lists[k].size());
+        depth = std::max(depth, lists[k].size());
     }
     void* fn = mega_kernel(kprec(prec));
     int per_sm = 0;
@@ -156,11 +156,11 @@ gpue_status plan_mega(const BatchRun& r, int prec, int s0, int s1, ArgSink& sink
         per_sm = 1;
     // work items of about 32K points, fewer when the solves are too few to
     // give every resident CTA work (a converged batch's tail)
-    double round_pts = 0;
-    for (int k = 0; k < ns; ++k) round_pts += (double)r.ctx[solves[k]]->N;
+    double layer_pts = 0;  // points of one pass over all solves
+    for (int k = 0; k < ns; ++k) layer_pts += (double)r.ctx[solves[k]]->N;
     const long item_pts =
-        std::max(2048L, std::min(32768L, (long)(round_pts / ((double)per_sm * c0->sms))));
-    // pass instances, round-major, cut into items; argument blocks stored once
+        std::max(2048L, std::min(32768L, (long)(layer_pts / ((double)per_sm * c0->sms))));
+    // pass instances by pass index, cut into items; argument blocks stored once
     // per content
     std::vector<MegaPass> inst;
     std::vector<int> item_pass;
@@ -169,7 +169,7 @@ gpue_status plan_mega(const BatchRun& r, int prec, int s0, int s1, ArgSink& sink
     std::vector<int> last(ns, -1);
     long start = 0;
     size_t smem = 2 * (kMegaThreads / 32) * sizeof(double);
-    for (size_t rd = 0; rd < rounds; ++rd) {
+    for (size_t rd = 0; rd < depth; ++rd) {
         for (int k = 0; k < ns; ++k) {
             if (rd >= lists[k].size()) continue;
             gpue_ctx* c = r.ctx[solves[k]];

@@ -3,8 +3,8 @@
 //
 // A segment of a batched run (the time steps up to the next energy check) is
 // a list of pass instances: pass r of solve s, for every solve and every
-// round r of its pass list (its own schedule: 2D or 3D, gauge or not).  The
-// instances are ordered round-major (round 0 of every solve, then round 1, ...)
+// pass r of its pass list (its own schedule: 2D or 3D, gauge or not).  The
+// instances are ordered by pass index (pass 0 of every solve, then pass 1, ...)
 // and cut into work items of `chunk` consecutive tiles (about 32K points), the
 // items numbered consecutively: a ticket, mapped to its instance by a table.
 // One launch of resident CTAs walks the tickets with an atomic counter; before

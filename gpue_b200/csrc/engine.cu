@@ -982,10 +982,8 @@ void destroy_graphs(gpue_ctx* c) {
 
 // ------------------------------------------------------------- autotune --
 
-// Mean device time of one FFT round-trip pass (forward then inverse along
-// the axis) over a copy of the state, with the current launch shape.
 // Device time of a few steps of this context's own schedule (the time kind
-// its tables are built for), so a candidate launch shape is judged by the
+// its tables are built for), so a candidate launch shape is compared on the
 // passes it will run, phases and reductions included.  The state and the
 // scalar slots are saved first and put back after.
 gpue_status time_steps(gpue_ctx* c, int prec, float* us) {
