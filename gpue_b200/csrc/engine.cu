@@ -459,6 +459,7 @@ gpue_status plan_xy(gpue_ctx* c, int prec) {
     gpue_status st = alloc_counters(c, xc.ctr);
     if (st) return st;
     if (const char* lag = std::getenv("GPUE_XY_LAG")) xc.ctr.lag = std::max(1, std::atoi(lag));
+    if (const char* w = std::getenv("GPUE_TEST_PLANE_WAIT")) xc.ctr.wait_extra = std::max(0, std::atoi(w));
     const long tiles = 2L * (n / 16) * c->ax[2].n;
     xc.blocks = (int)std::min<long>((long)per_sm * c->sms, tiles);
     xc.k = k;
@@ -1924,7 +1925,7 @@ gpue_status gpue_evolve(gpue_ctx* c, int32_t nsteps, int32_t gstate,
     CK(cudaEventSynchronize(c->ev1));
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
-    if (c->plane[c->prec].k) {
+    if (c->plane[c->prec].k || c->xy[c->prec].k || c->zpass[c->prec].k) {
         int gave_up = 0;
         CK(cudaMemcpy(&gave_up, c->dflags + 3, sizeof gave_up, cudaMemcpyDeviceToHost));
         if (gave_up) {

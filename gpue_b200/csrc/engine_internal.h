@@ -76,9 +76,14 @@ struct TSCounters {
     void* mem = nullptr;
     size_t bytes = 0;
     int lag = 64;  // XY pass: planes between a plane's x-tiles and its y-tiles
+    // XY pass: x-tiles beyond a plane's own that its y-tiles wait for: 0, or
+    // (GPUE_TEST_PLANE_WAIT, for tests only) more than ever come, so every
+    // such wait runs out and the run reports GPUE_ERR_TIMEOUT
+    int wait_extra = 0;
     XYCounters dev() const {
         XYCounters k;
         k.lag = lag;
+        k.wait_extra = wait_extra;
         k.ticket = static_cast<unsigned long long*>(mem);
         k.finish = reinterpret_cast<unsigned*>(static_cast<char*>(mem) + 8);
         k.done_x = reinterpret_cast<int*>(static_cast<char*>(mem) + 16);

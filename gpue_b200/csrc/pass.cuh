@@ -119,6 +119,7 @@ struct XYCounters {
     unsigned* finish;            // CTAs finished
     int* done_x;                 // [nz] x-tiles stored per plane (XY pass)
     int lag;                     // XY pass: planes between a plane's x-tiles and y-tiles
+    int wait_extra;              // XY pass: 0; > 0 only to test the bounded plane wait
 };
 
 // ------------------------------------------------------- FP64 reductions --

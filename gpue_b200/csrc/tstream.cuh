@@ -137,6 +137,14 @@ __device__ __forceinline__ void red_release_add(int* p, int v) {
     asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// Nanoseconds of the GPU's global timer: the bound of the plane wait.
+__device__ __forceinline__ uint64_t gpu_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+constexpr uint64_t kPlaneWaitNs = 1000000000ull;  // a y-tile waits at most 1 s for its plane
+
 __device__ __forceinline__ void mbar_arrive(uint64_t* b) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(b)) : "memory");
 }
@@ -212,6 +220,7 @@ __global__ void __launch_bounds__(TSShape<T, N, RA, RB, P, RC>::THREADS, 2)
         // ------------------------------------------------------ producer
         if (lane == 0) {
             const int lag = k.lag < 1 ? 1 : k.lag < nz ? k.lag : nz;
+            const int need = xi + k.wait_extra;  // x-tiles a plane's y-tiles wait for
             const long total = KIND == TS_Z ? (long)yi * a.ny : (long)nz * (xi + yi);
             // per landing buffer: its ticket and tile, whether its load waits
             // for a plane, the parity of its next done phase, the phases begun
@@ -282,7 +291,7 @@ __global__ void __launch_bounds__(TSShape<T, N, RA, RB, P, RC>::THREADS, 2)
                 }
                 slot[b] = make_int4(m.kind, m.z, m.tile, 0);
                 if (m.kind == TILE_Y && !known_ready(m.z)) {
-                    if (ld_acquire(k.done_x + m.z) < xi) {
+                    if (ld_acquire(k.done_x + m.z) < need) {
                         m.pend = true;
                         return;
                     }
@@ -298,9 +307,9 @@ __global__ void __launch_bounds__(TSShape<T, N, RA, RB, P, RC>::THREADS, 2)
                 if (m.pend) {
                     // every tile held with a smaller ticket is stored and
                     // counted (x-tiles are counted as their store completes)
-                    unsigned polls = 0;
-                    while (ld_acquire(k.done_x + m.z) < xi) {
-                        if (++polls >= kPlaneWaitPolls) {
+                    const uint64_t t0 = gpu_ns();
+                    while (ld_acquire(k.done_x + m.z) < need) {
+                        if (gpu_ns() - t0 > kPlaneWaitNs) {
                             ok = false;
                             break;
                         }
