@@ -299,8 +299,9 @@ class Solver:
         _check(lib().gpue_ctx_create(C.byref(params), C.byref(h)))
         self._h = h
         d = params.dimnum
-        n = params.xDim
-        self.shape = (n, n, n) if d == 3 else (n, n)
+        # [z, y, x], x fastest
+        self.shape = ((params.zDim, params.yDim, params.xDim) if d == 3
+                      else (params.yDim, params.xDim))
         self.precision = params.precision
 
     def close(self):

@@ -126,3 +126,4 @@ def test_time_passes_reports_the_step_and_leaves_the_state(gstate):
         u.evolve(4, gstate, step_offset=2)
         a, b = s.get_wfc(), u.get_wfc()
         assert np.max(np.abs(a - b)) <= 1e-6 * np.max(np.abs(b))
+
